@@ -1,0 +1,345 @@
+"""dumato_b200 - B200-native warp-centric subgraph enumeration (k-clique and k-motif counting).
+
+Python binding of the C ABI in include/dumato_b200.h (libdmb200.so, built in-tree by
+``python -m dumato_b200.build``). The binding is a thin ctypes layer: every counting call
+runs the library's sm_100a kernels; there is no CPU path, and a missing library or device
+raises instead of falling back.
+
+Reference correspondence (DuMato project root):
+    Graph.load_edgelist   - Graph::Graph(const char*)            src/main/Graph.cpp:17-54
+    count_cliques         - clique driver + outputAggregateCounter src/main/clique_PA.cu:34-130
+    count_motifs          - motif driver + outputAggregatePattern  src/main/motifs_DM_WCLB.cu:38-140
+    Dictionary.load_csv   - QuickMapping::QuickMapping(int k)      src/main/QuickMapping.cpp:5-45
+    Options(threads, block_size, donations_per_warp, threshold)
+                          - argv[3..6] of both drivers             src/main/clique_PA.cu:54-63
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass, field
+from pathlib import Path
+from typing import Optional, Sequence
+
+import numpy as np
+
+_PKG = Path(__file__).resolve().parent
+LIB_PATH = _PKG / "libdmb200.so"
+
+DM_OK = 0
+STATUS_NAMES = {
+    -1: "DM_EINVAL", -2: "DM_EIO", -3: "DM_EFORMAT", -4: "DM_ENOMEM", -5: "DM_ENODEVICE",
+    -6: "DM_ECUDA", -7: "DM_ETIMEOUT", -8: "DM_EOVERFLOW",
+}
+
+GEN_ER, GEN_CHUNG_LU, GEN_RMAT = 0, 1, 2
+MODE_AUTO, MODE_LIST, MODE_BITMAP = 0, 1, 2
+SCHED_PLAIN, SCHED_LEARNED, SCHED_ID = 0, 1, 2
+
+
+class DMError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+
+
+class _GenParams(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int32), ("n", ctypes.c_int32), ("m", ctypes.c_int64),
+                ("gamma", ctypes.c_double), ("dmax", ctypes.c_double), ("a", ctypes.c_double),
+                ("b", ctypes.c_double), ("c", ctypes.c_double), ("seed", ctypes.c_uint64)]
+
+
+class _GraphInfo(ctypes.Structure):
+    _fields_ = [("n_vertices", ctypes.c_int32), ("n_edges", ctypes.c_int64), ("max_degree", ctypes.c_int32),
+                ("max_out_degree", ctypes.c_int32), ("n_self_loops", ctypes.c_int64),
+                ("n_input_pairs", ctypes.c_int64)]
+
+
+class _Opts(ctypes.Structure):
+    _fields_ = [("struct_size", ctypes.c_int32), ("device", ctypes.c_int32), ("stream", ctypes.c_uint64),
+                ("threads", ctypes.c_int32), ("block_size", ctypes.c_int32),
+                ("donations_per_warp", ctypes.c_int32), ("threshold", ctypes.c_int32),
+                ("vwarp", ctypes.c_int32), ("mode", ctypes.c_int32), ("scheduler", ctypes.c_int32),
+                ("rank", ctypes.c_int32), ("world_size", ctypes.c_int32), ("timeout_ms", ctypes.c_int32),
+                ("predictor", ctypes.c_void_p)]
+
+
+class _Stats(ctypes.Structure):
+    _fields_ = [("kernel_ms", ctypes.c_double), ("prep_ms", ctypes.c_double), ("tasks", ctypes.c_uint64),
+                ("donations", ctypes.c_uint64), ("idle_polls", ctypes.c_uint64), ("nodes", ctypes.c_uint64),
+                ("mode_used", ctypes.c_int32), ("vwarp_used", ctypes.c_int32), ("grid", ctypes.c_int32),
+                ("block", ctypes.c_int32), ("kernel_launches", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+
+
+_P = ctypes.c_void_p
+_SIGNATURES = {
+    "dm_abi_version": (ctypes.c_int, []),
+    "dm_last_error": (ctypes.c_char_p, []),
+    "dm_device_count": (ctypes.c_int, []),
+    "dm_graph_load_edgelist": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(_P)]),
+    "dm_graph_from_edges": (ctypes.c_int, [_P, _P, ctypes.c_int64, ctypes.c_int32, ctypes.POINTER(_P)]),
+    "dm_graph_generate": (ctypes.c_int, [ctypes.POINTER(_GenParams), ctypes.POINTER(_P)]),
+    "dm_graph_info_get": (ctypes.c_int, [_P, ctypes.POINTER(_GraphInfo)]),
+    "dm_graph_edges": (ctypes.c_int, [_P, _P, _P]),
+    "dm_graph_csr": (ctypes.c_int, [_P, _P, _P]),
+    "dm_graph_write_edgelist": (ctypes.c_int, [_P, ctypes.c_char_p]),
+    "dm_graph_free": (None, [_P]),
+    "dm_graph_release_device": (ctypes.c_int, [_P]),
+    "dm_dictionary_generate": (ctypes.c_int, [ctypes.c_int32, ctypes.POINTER(_P)]),
+    "dm_dictionary_load_csv": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(_P)]),
+    "dm_dictionary_write_csv": (ctypes.c_int, [_P, ctypes.c_char_p]),
+    "dm_dictionary_shape": (ctypes.c_int, [_P, _P, _P, _P]),
+    "dm_dictionary_tables": (ctypes.c_int, [_P, _P, _P]),
+    "dm_dictionary_connected": (ctypes.c_int, [_P, _P]),
+    "dm_dictionary_free": (None, [_P]),
+    "dm_count_cliques": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.POINTER(_Opts), _P, ctypes.POINTER(_Stats)]),
+    "dm_count_motifs": (ctypes.c_int, [_P, ctypes.c_int32, _P, ctypes.POINTER(_Opts), _P, ctypes.POINTER(_Stats)]),
+}
+
+_lib: Optional[ctypes.CDLL] = None
+
+
+def lib() -> ctypes.CDLL:
+    """Loads libdmb200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise ImportError(f"{LIB_PATH} is missing: run `python -m dumato_b200.build` first")
+        L = ctypes.CDLL(str(LIB_PATH))
+        for name, (res, args) in _SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def exported_symbols() -> list[str]:
+    return list(_SIGNATURES)
+
+
+def _check(rc: int) -> None:
+    if rc != DM_OK:
+        msg = lib().dm_last_error()
+        raise DMError(rc, msg.decode() if msg else "")
+
+
+def _ptr(a: np.ndarray) -> ctypes.c_void_p:
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+def device_count() -> int:
+    return lib().dm_device_count()
+
+
+@dataclass
+class GraphInfo:
+    n_vertices: int
+    n_edges: int
+    max_degree: int
+    max_out_degree: int
+    n_self_loops: int
+    n_input_pairs: int
+
+
+class Graph:
+    """An undirected, unlabeled graph (ids in [0, V-1], duplicates merged, self-loops dropped)."""
+
+    def __init__(self, handle: ctypes.c_void_p):
+        self._h = handle
+
+    @classmethod
+    def load_edgelist(cls, path: str | os.PathLike) -> "Graph":
+        h = _P()
+        _check(lib().dm_graph_load_edgelist(str(path).encode(), ctypes.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def from_edges(cls, src: Sequence[int], dst: Sequence[int], n_vertices: int = 0) -> "Graph":
+        s = np.ascontiguousarray(src, dtype=np.int32)
+        d = np.ascontiguousarray(dst, dtype=np.int32)
+        if s.shape != d.shape:
+            raise ValueError("src and dst differ in length")
+        h = _P()
+        _check(lib().dm_graph_from_edges(_ptr(s), _ptr(d), s.size, int(n_vertices), ctypes.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def generate(cls, kind: int, n: int, m: int, seed: int, gamma: float = 2.1, dmax: float = 500.0,
+                 a: float = 0.57, b: float = 0.19, c: float = 0.19) -> "Graph":
+        p = _GenParams(kind=kind, n=n, m=m, gamma=gamma, dmax=dmax, a=a, b=b, c=c, seed=seed)
+        h = _P()
+        _check(lib().dm_graph_generate(ctypes.byref(p), ctypes.byref(h)))
+        return cls(h)
+
+    @property
+    def handle(self) -> ctypes.c_void_p:
+        if self._h is None:
+            raise ValueError("graph was freed")
+        return self._h
+
+    def info(self) -> GraphInfo:
+        i = _GraphInfo()
+        _check(lib().dm_graph_info_get(self.handle, ctypes.byref(i)))
+        return GraphInfo(i.n_vertices, i.n_edges, i.max_degree, i.max_out_degree, i.n_self_loops, i.n_input_pairs)
+
+    def edges(self) -> tuple[np.ndarray, np.ndarray]:
+        m = self.info().n_edges
+        u = np.empty(m, np.int32)
+        v = np.empty(m, np.int32)
+        _check(lib().dm_graph_edges(self.handle, _ptr(u), _ptr(v)))
+        return u, v
+
+    def csr(self) -> tuple[np.ndarray, np.ndarray]:
+        inf = self.info()
+        off = np.empty(inf.n_vertices + 1, np.int64)
+        adj = np.empty(2 * inf.n_edges, np.int32)
+        _check(lib().dm_graph_csr(self.handle, _ptr(off), _ptr(adj)))
+        return off, adj
+
+    def write_edgelist(self, path: str | os.PathLike) -> None:
+        _check(lib().dm_graph_write_edgelist(self.handle, str(path).encode()))
+
+    def release_device(self) -> None:
+        _check(lib().dm_graph_release_device(self.handle))
+
+    def free(self) -> None:
+        if self._h is not None:
+            lib().dm_graph_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+class Dictionary:
+    """quick code -> canonical class table for k-vertex motifs (k in 3..7)."""
+
+    def __init__(self, handle: ctypes.c_void_p):
+        self._h = handle
+
+    @classmethod
+    def generate(cls, k: int) -> "Dictionary":
+        h = _P()
+        _check(lib().dm_dictionary_generate(int(k), ctypes.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def load_csv(cls, path: str | os.PathLike) -> "Dictionary":
+        h = _P()
+        _check(lib().dm_dictionary_load_csv(str(path).encode(), ctypes.byref(h)))
+        return cls(h)
+
+    @property
+    def handle(self) -> ctypes.c_void_p:
+        return self._h
+
+    def shape(self) -> tuple[int, int, int]:
+        k = ctypes.c_int32()
+        nq = ctypes.c_int64()
+        nc = ctypes.c_int32()
+        _check(lib().dm_dictionary_shape(self._h, ctypes.byref(k), ctypes.byref(nq), ctypes.byref(nc)))
+        return k.value, nq.value, nc.value
+
+    @property
+    def k(self) -> int:
+        return self.shape()[0]
+
+    @property
+    def n_classes(self) -> int:
+        return self.shape()[2]
+
+    def tables(self) -> tuple[np.ndarray, np.ndarray]:
+        _, nq, nc = self.shape()
+        q2c = np.empty(nq, np.int32)
+        code = np.empty(nc, np.uint64)
+        _check(lib().dm_dictionary_tables(self._h, _ptr(q2c), _ptr(code)))
+        return q2c, code
+
+    def connected(self) -> np.ndarray:
+        nc = self.n_classes
+        out = np.empty(nc, np.uint8)
+        _check(lib().dm_dictionary_connected(self._h, _ptr(out)))
+        return out.astype(bool)
+
+    def write_csv(self, path: str | os.PathLike) -> None:
+        _check(lib().dm_dictionary_write_csv(self._h, str(path).encode()))
+
+    def __del__(self):
+        try:
+            if self._h is not None:
+                lib().dm_dictionary_free(self._h)
+                self._h = None
+        except Exception:
+            pass
+
+
+@dataclass
+class Options:
+    """Engine options; threads/block_size/donations_per_warp/threshold are the reference's
+    positional CLI arguments 3..6 (src/main/clique_PA.cu:54-63)."""
+    device: int = -1
+    stream: int = 0
+    threads: int = 0
+    block_size: int = 0
+    donations_per_warp: int = 16
+    threshold: int = 30
+    vwarp: int = 0
+    mode: int = MODE_AUTO
+    scheduler: int = SCHED_PLAIN
+    rank: int = 0
+    world_size: int = 1
+    timeout_ms: int = 2000
+    predictor: Optional[int] = None
+
+    def to_c(self) -> _Opts:
+        return _Opts(struct_size=ctypes.sizeof(_Opts), device=self.device, stream=self.stream,
+                     threads=self.threads, block_size=self.block_size,
+                     donations_per_warp=self.donations_per_warp, threshold=self.threshold, vwarp=self.vwarp,
+                     mode=self.mode, scheduler=self.scheduler, rank=self.rank, world_size=self.world_size,
+                     timeout_ms=self.timeout_ms, predictor=self.predictor)
+
+
+@dataclass
+class Stats:
+    kernel_ms: float = 0.0
+    prep_ms: float = 0.0
+    tasks: int = 0
+    donations: int = 0
+    idle_polls: int = 0
+    nodes: int = 0
+    mode_used: int = 0
+    vwarp_used: int = 0
+    grid: int = 0
+    block: int = 0
+    kernel_launches: int = 0
+
+    @classmethod
+    def from_c(cls, s: _Stats) -> "Stats":
+        return cls(s.kernel_ms, s.prep_ms, s.tasks, s.donations, s.idle_polls, s.nodes, s.mode_used,
+                   s.vwarp_used, s.grid, s.block, s.kernel_launches)
+
+
+def count_cliques(g: Graph, k: int, opts: Optional[Options] = None) -> tuple[int, Stats]:
+    """Number of k-cliques of g (exact uint64), computed on the GPU."""
+    o = (opts or Options()).to_c()
+    out = ctypes.c_uint64()
+    st = _Stats()
+    _check(lib().dm_count_cliques(g.handle, int(k), ctypes.byref(o), ctypes.byref(out), ctypes.byref(st)))
+    return out.value, Stats.from_c(st)
+
+
+def count_motifs(g: Graph, k: int, dictionary: Optional[Dictionary] = None,
+                 opts: Optional[Options] = None) -> tuple[np.ndarray, Stats]:
+    """Connected induced k-subgraph counts per dictionary class (uint64[n_classes])."""
+    d = dictionary or Dictionary.generate(k)
+    if d.k != k:
+        raise ValueError(f"dictionary is for k={d.k}, asked for k={k}")
+    o = (opts or Options()).to_c()
+    out = np.zeros(d.n_classes, np.uint64)
+    st = _Stats()
+    _check(lib().dm_count_motifs(g.handle, int(k), d.handle, ctypes.byref(o), _ptr(out), ctypes.byref(st)))
+    return out, Stats.from_c(st)

@@ -1,0 +1,24 @@
+"""Seeded synthetic workloads standing in for the benchmark datasets (sizes from the
+five benchmark configurations). Generator parameters are fixed here so tests, bench and
+fixtures agree on the exact graphs."""
+from __future__ import annotations
+
+CONFIGS = {
+    # Erdos-Renyi G(n, m): 2,000 vertices, 10,000 undirected edges
+    "er2k": dict(kind=0, n=2000, m=10_000),
+    # Chung-Lu power law: ~18,700 vertices, ~198,000 edges, exponent 2.1, max degree ~500
+    "chunglu18k": dict(kind=1, n=18_700, m=198_000, gamma=2.1, dmax=500.0),
+    # R-MAT (.57,.19,.19,.05): ids < 170,000 -> ~98.6k touched vertices, 1.08M edges
+    "rmat100k": dict(kind=2, n=170_000, m=1_080_000, a=0.57, b=0.19, c=0.19),
+    # R-MAT (.57,.19,.19,.05): ids < 1,400,000 -> ~321k touched vertices, 1.05M edges
+    "rmat317k": dict(kind=2, n=1_400_000, m=1_050_000, a=0.57, b=0.19, c=0.19),
+}
+
+
+def make(name: str, seed: int = 1):
+    """Generates the named workload graph (deterministic for a given seed)."""
+    from . import Graph
+
+    p = dict(CONFIGS[name])
+    kind = p.pop("kind")
+    return Graph.generate(kind, p.pop("n"), p.pop("m"), seed=seed, **p)

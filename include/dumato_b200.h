@@ -1,0 +1,167 @@
+/*
+ * dumato_b200.h - C ABI of the B200-native warp-centric subgraph enumeration engine.
+ *
+ * This is the drop-in boundary for DuMato's clique and motif counting path.
+ * Every entry point takes plain pointers and sizes; no C++ or framework types cross it.
+ * All functions return DM_OK (0) on success and a negative DM_E* status on failure;
+ * dm_last_error() then gives a one-line message for the calling thread.
+ * The library never calls exit() (unlike the reference's gpuErrorCheck,
+ * src/main/Structs.cu:7-16) and never falls back to a CPU path: counting entry points
+ * return DM_ENODEVICE when no CUDA device can be used.
+ *
+ * Reference interfaces replaced (paths are relative to the DuMato project root):
+ *   Graph::Graph(const char*)            src/main/Graph.cpp:17-54      -> dm_graph_load_edgelist
+ *   DuMatoCPU CSR build                  src/main/DuMatoCPU.cu:94-108  -> dm_graph_* (internal CSR)
+ *   DuMatoCPU::DuMatoCPU(...)            src/main/DuMatoCPU.h:46       -> dm_opts (threads, blockSize,
+ *                                                                          donationsPerWarp, threshold)
+ *   DuMatoCPU::runKernel/waitKernel      src/main/DuMatoCPU.cu:316-326 -> dm_count_cliques / dm_count_motifs
+ *   clique kernel + outputAggregateCounter  src/main/clique_PA.cu:9-32,
+ *                                        src/main/DuMatoCPU.cu:360-362 -> dm_count_cliques
+ *   motifs kernel + outputAggregatePattern  src/main/motifs_DM_WCLB.cu:9-36,
+ *                                        src/main/DuMatoCPU.cu:364-384 -> dm_count_motifs
+ *   QuickMapping::QuickMapping(int k)    src/main/QuickMapping.cpp:5-45 -> dm_dictionary_load_csv
+ *   nauty-based dictionary generation    src/motifs_DM_DFS/Manager.cpp:1067-1118
+ *                                                                       -> dm_dictionary_generate
+ */
+#ifndef DUMATO_B200_H
+#define DUMATO_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DM_ABI_VERSION 1
+
+#if defined(__GNUC__)
+#define DM_API __attribute__((visibility("default")))
+#else
+#define DM_API
+#endif
+
+/* status codes */
+#define DM_OK 0
+#define DM_EINVAL (-1)     /* bad argument (k out of range, null pointer, bad options) */
+#define DM_EIO (-2)        /* file missing or unreadable */
+#define DM_EFORMAT (-3)    /* malformed edgelist or dictionary */
+#define DM_ENOMEM (-4)     /* host or device allocation failed */
+#define DM_ENODEVICE (-5)  /* no usable CUDA device */
+#define DM_ECUDA (-6)      /* a CUDA call failed */
+#define DM_ETIMEOUT (-7)   /* a bounded device-side wait gave up (error word set by a kernel) */
+#define DM_EOVERFLOW (-8)  /* a device-side capacity bound was exceeded */
+
+typedef struct dm_graph dm_graph;
+typedef struct dm_dictionary dm_dictionary;
+
+/* Graph generators (seeded, deterministic on every platform). */
+#define DM_GEN_ER 0        /* G(n, m): m distinct undirected pairs, no self-loops */
+#define DM_GEN_CHUNG_LU 1  /* power-law weights w_i ~ (1 + i/i0)^(-1/(gamma-1)) capped at dmax */
+#define DM_GEN_RMAT 2      /* R-MAT (a, b, c, 1-a-b-c), trimmed to ids < n, touched ids relabelled */
+
+typedef struct dm_gen_params {
+  int32_t kind;       /* DM_GEN_* */
+  int32_t n;          /* vertices (R-MAT: id bound before compaction) */
+  int64_t m;          /* distinct undirected edges wanted */
+  double gamma;       /* Chung-Lu degree exponent */
+  double dmax;        /* Chung-Lu weight cap */
+  double a, b, c;     /* R-MAT quadrant probabilities */
+  uint64_t seed;
+} dm_gen_params;
+
+typedef struct dm_graph_info {
+  int32_t n_vertices;      /* max id + 1 (isolated ids kept, as Graph.cpp:34-38) */
+  int64_t n_edges;         /* distinct undirected edges, self-loops dropped */
+  int32_t max_degree;
+  int32_t max_out_degree;  /* in the degree-ordered orientation used for cliques */
+  int64_t n_self_loops;    /* self-loops seen in the input and dropped */
+  int64_t n_input_pairs;   /* pairs read or generated before dedup */
+} dm_graph_info;
+
+/* Engine options. Zero-initialise and set struct_size = sizeof(dm_opts). */
+#define DM_MODE_AUTO 0
+#define DM_MODE_LIST 1     /* sorted-list intersection with warp ballot compaction */
+#define DM_MODE_BITMAP 2   /* per-root local adjacency bitmaps */
+
+#define DM_SCHED_PLAIN 0   /* roots in descending degree order + device donation */
+#define DM_SCHED_LEARNED 1 /* roots ordered by the work predictor (needs a trained predictor) */
+#define DM_SCHED_ID 2      /* roots in id order (the reference's striping order) */
+
+typedef struct dm_opts {
+  int32_t struct_size;
+  int32_t device;              /* CUDA ordinal; -1 = current device */
+  uint64_t stream;             /* cudaStream_t to launch on; 0 = the library's own stream */
+  int32_t threads;             /* reference argv[3]: total GPU threads (0 = persistent default) */
+  int32_t block_size;          /* reference argv[4]: threads per block (0 = 256) */
+  int32_t donations_per_warp;  /* reference argv[5]: donation batch bound (0 = 16) */
+  int32_t threshold;           /* reference argv[6]: idle-warp percentage that triggers donation;
+                                  >= 100 disables donation (clique_PA.cu:78) */
+  int32_t vwarp;               /* virtual-warp width 0 (auto), 8, 16 or 32 */
+  int32_t mode;                /* DM_MODE_* */
+  int32_t scheduler;           /* DM_SCHED_* */
+  int32_t rank;                /* root shard: this process counts roots r with r % world == rank */
+  int32_t world_size;          /* 0 or 1 = unsharded */
+  int32_t timeout_ms;          /* bound on every device-side wait (0 = 2000 ms) */
+  const void* predictor;       /* dm_predictor* for DM_SCHED_LEARNED, else NULL */
+} dm_opts;
+
+typedef struct dm_stats {
+  double kernel_ms;            /* device time of the counting kernels (CUDA events) */
+  double prep_ms;              /* device time of graph upload/orientation/task ordering */
+  uint64_t tasks;              /* root (or donated-prefix) tasks executed */
+  uint64_t donations;          /* prefixes donated between warps */
+  uint64_t idle_polls;         /* polls by warps that found no work */
+  uint64_t nodes;              /* DFS nodes expanded (extend calls) */
+  int32_t mode_used;           /* DM_MODE_* actually run */
+  int32_t vwarp_used;
+  int32_t grid;                /* CTAs launched */
+  int32_t block;               /* threads per CTA */
+  int32_t kernel_launches;     /* kernels of this library launched for the call */
+  int32_t reserved;
+} dm_stats;
+
+/* ---- version / errors ---- */
+DM_API int dm_abi_version(void);
+DM_API const char* dm_last_error(void);
+DM_API int dm_device_count(void);
+
+/* ---- graphs ---- */
+DM_API int dm_graph_load_edgelist(const char* path, dm_graph** out);
+DM_API int dm_graph_from_edges(const int32_t* src, const int32_t* dst, int64_t n_pairs,
+                        int32_t n_vertices, dm_graph** out);
+DM_API int dm_graph_generate(const dm_gen_params* params, dm_graph** out);
+DM_API int dm_graph_info_get(const dm_graph* g, dm_graph_info* info);
+/* Distinct undirected edges as (u < v) pairs, sorted; arrays of length info.n_edges. */
+DM_API int dm_graph_edges(const dm_graph* g, int32_t* u, int32_t* v);
+/* Undirected CSR: offsets[n+1] (int64), adjacency[2m] sorted ascending per row. */
+DM_API int dm_graph_csr(const dm_graph* g, int64_t* offsets, int32_t* adjacency);
+DM_API int dm_graph_write_edgelist(const dm_graph* g, const char* path);
+DM_API void dm_graph_free(dm_graph* g);
+
+/* ---- canonical-class dictionaries (quick code -> class) ---- */
+DM_API int dm_dictionary_generate(int32_t k, dm_dictionary** out);
+DM_API int dm_dictionary_load_csv(const char* path, dm_dictionary** out);
+DM_API int dm_dictionary_write_csv(const dm_dictionary* d, const char* path);
+/* k, number of quick codes (2^(k(k-1)/2-1)), number of classes */
+DM_API int dm_dictionary_shape(const dm_dictionary* d, int32_t* k, int64_t* n_quicks, int32_t* n_classes);
+/* quick_to_class[n_quicks] and class_code[n_classes] (the class's global code) */
+DM_API int dm_dictionary_tables(const dm_dictionary* d, int32_t* quick_to_class, uint64_t* class_code);
+/* 1 if the class is a connected graph, else 0; connected[n_classes] */
+DM_API int dm_dictionary_connected(const dm_dictionary* d, uint8_t* connected);
+DM_API void dm_dictionary_free(dm_dictionary* d);
+
+/* ---- counting (GPU only) ---- */
+/* Number of k-cliques, k in [2, 12]. */
+DM_API int dm_count_cliques(dm_graph* g, int32_t k, const dm_opts* opts, uint64_t* count, dm_stats* stats);
+/* Connected induced k-vertex subgraphs per class of dict (k in [3, 7]).
+   class_counts has n_classes entries (dm_dictionary_shape). */
+DM_API int dm_count_motifs(dm_graph* g, int32_t k, const dm_dictionary* dict, const dm_opts* opts,
+                    uint64_t* class_counts, dm_stats* stats);
+
+/* Release this library's device copies of g on its device (host CSR stays). */
+DM_API int dm_graph_release_device(dm_graph* g);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DUMATO_B200_H */

@@ -1,0 +1,127 @@
+"""ctypes binding of the CPU oracle (oracle/liboracle.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and bench.py's
+cpu_baseline / reference legs, never by the dumato_b200 package.
+"""
+from __future__ import annotations
+
+import ctypes
+import subprocess
+from pathlib import Path
+from typing import Optional
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "liboracle.so"
+_lib: Optional[ctypes.CDLL] = None
+_P = ctypes.c_void_p
+
+
+def build() -> Path:
+    subprocess.run(["make", "-s", "-C", str(HERE), "liboracle.so"], check=True)
+    return LIB_PATH
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            build()
+        L = ctypes.CDLL(str(LIB_PATH))
+        sig = {
+            "oracle_graph_from_pairs": (_P, [_P, _P, ctypes.c_int64]),
+            "oracle_graph_load": (_P, [ctypes.c_char_p]),
+            "oracle_graph_free": (None, [_P]),
+            "oracle_graph_n": (ctypes.c_int32, [_P]),
+            "oracle_graph_m": (ctypes.c_int64, [_P]),
+            "oracle_graph_maxdeg": (ctypes.c_int32, [_P]),
+            "oracle_clique_dfs": (ctypes.c_uint64, [_P, ctypes.c_int, ctypes.c_int]),
+            "oracle_clique_dfs_range": (ctypes.c_uint64, [_P, ctypes.c_int, ctypes.c_int32, ctypes.c_int32, ctypes.c_int]),
+            "oracle_clique_brute": (ctypes.c_uint64, [_P, ctypes.c_int]),
+            "oracle_clique_dag_bytes": (ctypes.c_uint64, [_P, ctypes.c_int, _P, ctypes.c_int]),
+            "oracle_motifs": (ctypes.c_int, [_P, ctypes.c_int, _P, ctypes.c_int32, _P, ctypes.c_int]),
+            "oracle_motifs_range": (ctypes.c_int, [_P, ctypes.c_int, _P, ctypes.c_int32, _P, ctypes.c_int32,
+                                                   ctypes.c_int32, ctypes.c_int, _P]),
+            "oracle_motifs_brute": (ctypes.c_int, [_P, ctypes.c_int, _P, ctypes.c_int32, _P]),
+        }
+        for name, (res, args) in sig.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+class OracleGraph:
+    """The reference reader's view of a graph (set adjacency, self-loops kept)."""
+
+    def __init__(self, h):
+        if not h:
+            raise ValueError("oracle could not read the graph")
+        self.h = h
+
+    @classmethod
+    def from_pairs(cls, src, dst) -> "OracleGraph":
+        s = np.ascontiguousarray(src, dtype=np.int32)
+        d = np.ascontiguousarray(dst, dtype=np.int32)
+        return cls(lib().oracle_graph_from_pairs(s.ctypes.data, d.ctypes.data, s.size))
+
+    @classmethod
+    def load(cls, path) -> "OracleGraph":
+        return cls(lib().oracle_graph_load(str(path).encode()))
+
+    @property
+    def n(self) -> int:
+        return lib().oracle_graph_n(self.h)
+
+    @property
+    def m(self) -> int:
+        return lib().oracle_graph_m(self.h)
+
+    @property
+    def maxdeg(self) -> int:
+        return lib().oracle_graph_maxdeg(self.h)
+
+    def __del__(self):
+        try:
+            lib().oracle_graph_free(self.h)
+        except Exception:
+            pass
+
+
+def clique_dfs(g: OracleGraph, k: int, threads: int = 0, root_begin: int = 0, root_end: int = -1) -> int:
+    if root_end < 0:
+        root_end = g.n
+    return lib().oracle_clique_dfs_range(g.h, k, root_begin, root_end, threads)
+
+
+def clique_brute(g: OracleGraph, k: int) -> int:
+    return lib().oracle_clique_brute(g.h, k)
+
+
+def clique_dag_bytes(g: OracleGraph, k: int, threads: int = 0) -> tuple[int, int]:
+    b = ctypes.c_uint64()
+    c = lib().oracle_clique_dag_bytes(g.h, k, ctypes.byref(b), threads)
+    return c, b.value
+
+
+def motifs(g: OracleGraph, k: int, q2c: np.ndarray, n_classes: int, threads: int = 0,
+           root_begin: int = 0, root_end: int = -1, with_bytes: bool = False):
+    q = np.ascontiguousarray(q2c, dtype=np.int32)
+    hist = np.zeros(n_classes, np.uint64)
+    if root_end < 0:
+        root_end = g.n
+    b = ctypes.c_uint64()
+    rc = lib().oracle_motifs_range(g.h, k, q.ctypes.data, n_classes, hist.ctypes.data, root_begin, root_end, threads,
+                                   ctypes.byref(b) if with_bytes else None)
+    if rc != 0:
+        raise RuntimeError(f"oracle_motifs failed ({rc})")
+    return (hist, b.value) if with_bytes else hist
+
+
+def motifs_brute(g: OracleGraph, k: int, q2c: np.ndarray, n_classes: int) -> np.ndarray:
+    q = np.ascontiguousarray(q2c, dtype=np.int32)
+    hist = np.zeros(n_classes, np.uint64)
+    lib().oracle_motifs_brute(g.h, k, q.ctypes.data, n_classes, hist.ctypes.data)
+    return hist
