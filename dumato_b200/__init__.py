@@ -61,7 +61,7 @@ class _Opts(ctypes.Structure):
                 ("donations_per_warp", ctypes.c_int32), ("threshold", ctypes.c_int32),
                 ("vwarp", ctypes.c_int32), ("mode", ctypes.c_int32), ("scheduler", ctypes.c_int32),
                 ("rank", ctypes.c_int32), ("world_size", ctypes.c_int32), ("timeout_ms", ctypes.c_int32),
-                ("predictor", ctypes.c_void_p)]
+                ("predictor", ctypes.c_void_p), ("subtree_counts", ctypes.c_void_p)]
 
 
 class _Stats(ctypes.Structure):
@@ -286,21 +286,27 @@ class Options:
     threads: int = 0
     block_size: int = 0
     donations_per_warp: int = 16
-    threshold: int = 30
+    threshold: int = 0
     vwarp: int = 0
     mode: int = MODE_AUTO
     scheduler: int = SCHED_PLAIN
     rank: int = 0
     world_size: int = 1
-    timeout_ms: int = 2000
+    timeout_ms: int = 0
     predictor: Optional[int] = None
+    subtree_counts: Optional[np.ndarray] = None   # uint64[n_vertices], filled per root
 
     def to_c(self) -> _Opts:
+        st = None
+        if self.subtree_counts is not None:
+            if self.subtree_counts.dtype != np.uint64 or not self.subtree_counts.flags.c_contiguous:
+                raise ValueError("subtree_counts must be a contiguous uint64 array")
+            st = self.subtree_counts.ctypes.data
         return _Opts(struct_size=ctypes.sizeof(_Opts), device=self.device, stream=self.stream,
                      threads=self.threads, block_size=self.block_size,
                      donations_per_warp=self.donations_per_warp, threshold=self.threshold, vwarp=self.vwarp,
                      mode=self.mode, scheduler=self.scheduler, rank=self.rank, world_size=self.world_size,
-                     timeout_ms=self.timeout_ms, predictor=self.predictor)
+                     timeout_ms=self.timeout_ms, predictor=self.predictor, subtree_counts=st)
 
 
 @dataclass

@@ -1,29 +1,32 @@
-// k-clique counting kernels for sm_100a.
+// k-clique counting kernel for sm_100a.
 //
 // Semantics: the number of k-vertex cliques, each counted once, as the reference's clique
 // driver computes (src/main/clique_PA.cu:9-32 with extend_clique, DuMatoGPU.cu:1194-1220:
-// C_l = {u in N(v_l) : u > v_l} cap C_{l-1}, the leaf level adding |C_{k-2}|,
-// aggregate_counter DuMatoGPU.cu:1769-1771). The reference breaks symmetry by vertex id on
+// C_l = {u in N(v_l) : u > v_l} cap C_{l-1}, the leaf level adding |C_{k-2}| through
+// aggregate_counter, DuMatoGPU.cu:1769-1771). The reference breaks symmetry by vertex id on
 // the undirected graph; here the graph is oriented by (degree, id) rank, which counts the
-// same set of cliques with out-degrees bounded by O(sqrt(m)).
+// same cliques with out-degrees bounded by O(sqrt(m)).
 //
-// Three execution modes, chosen per root by its out-degree d (all produce exact counts):
-//   thread mode (d <= 128): the warp turns the root's out-neighbourhood into a local
-//       adjacency bitmap in shared memory (row c = out-neighbours of the c-th neighbour,
-//       as a d-bit set); each lane then runs its own DFS over 64-bit (or 128-bit) sets.
-//       extend = AND of two rows, compact = nothing (bit order is the candidate order),
+// One persistent launch runs every root. A root's work is split into items that lanes (or
+// warps) pull dynamically, and idle warps receive donated item ranges (lb.cuh):
+//   bitmap path (out-degree d <= 64*NWMAX, NWMAX <= 4): the warp builds the local
+//       adjacency bitmap of the root's out-neighbourhood L in shared memory (bit j of row i
+//       set iff L[j] in N+(L[i])). Items are the local edges (c1, c2); a lane takes an item
+//       and counts the (k-3)-cliques of row[c1] & row[c2] by its own DFS over 64-bit words:
+//       extend = AND of two rows, compact = nothing (bit order is candidate order),
 //       aggregate = popc at the last level.
-//   warp mode (128 < d <= 2048): same local bitmap in global scratch, one 32-bit word per
-//       lane (two for d > 1024), warp-cooperative DFS with ballot-based candidate pops.
-//   list mode (any d): the reference's list structure - per-level sorted candidate lists in
-//       a per-warp global arena, extended by binary-search intersection and ballot
-//       compaction (DuMatoGPU.cu:317-328 write), the leaf level counted without writing.
+//   list path (larger d, or DM_MODE_LIST): the reference's list structure. Items are the
+//       first-level candidates c1; the warp extends sorted candidate lists level by level in
+//       a per-warp global arena by binary-search intersection and ballot compaction
+//       (DuMatoGPU.cu:317-328 write), counting the leaf level without writing it.
+#include <algorithm>
 #include <climits>
 #include <cstdio>
 #include <string>
 
 #include "engine.hpp"
 #include "gpm.cuh"
+#include "lb.cuh"
 
 namespace dmb {
 
@@ -68,33 +71,58 @@ __device__ __forceinline__ unsigned long long count_rec(const Bits<NW>& S, const
   }
 }
 
-// Shared-memory bytes one warp needs in thread mode.
+// Position of the j-th (0-based) set bit of an NW-word row.
 template <int NW>
-__host__ __device__ constexpr size_t thread_warp_smem() {
-  return sizeof(uint32_t) * (64 * NW) * (2 * NW) + sizeof(int32_t) * (2 * 64 * NW + 4);
+__device__ __forceinline__ int select_bit(const uint64_t* row, int j) {
+#pragma unroll
+  for (int w = 0; w < NW; ++w) {
+    const uint64_t x = row[w];
+    const int pc = __popcll(x);
+    if (j < pc) {
+      const unsigned lo = (unsigned)x;
+      const int pl = __popc(lo);
+      if (j < pl) return w * 64 + (int)__fns(lo, 0, j + 1);
+      return w * 64 + 32 + (int)__fns((unsigned)(x >> 32), 0, j - pl + 1);
+    }
+    j -= pc;
+  }
+  return -1;
 }
 
-// Builds the local adjacency bitmap of the root's out-neighbourhood L[0..d):
-// bit j of row i is set iff L[j] is an out-neighbour of L[i]. The work is flattened over
-// all (i, neighbour) pairs so a warp stays busy when rows are short; membership in L is a
-// binary search in shared memory. Rows are zeroed by the caller.
-__device__ __forceinline__ void build_local_rows(const GraphView& g, const int32_t* sL, const int32_t* sP, int d,
-                                                 int total, uint32_t* rows, int row_words) {
-  const int lane = lane_id();
-  const int32_t maxL = sL[d - 1];
-  for (int f = lane; f < total; f += 32) {
-    int i = lower_bound(sP, 0, d + 1, f + 1) - 1;  // largest i with sP[i] <= f
-    const int u = sL[i];
-    const int32_t x = __ldg(g.adj + __ldg(g.row + u) + (f - sP[i]));
-    if (x <= maxL) {
-      int j = lower_bound(sL, i + 1, d, x);
-      if (j < d && sL[j] == x) {
-        uint32_t* w = rows + (size_t)i * row_words + (j >> 5);
-        atomicOr(w, 1u << (j & 31));
-      }
-    }
-  }
+// Shared memory of one warp for a launch whose bitmap roots need up to M words per row:
+// rows | L | prefix of out-degrees | prefix of row popcounts | item range | list stack.
+struct WarpLayout {
+  int rows, L, P, E, range, don, busy, hn, heavy, ptr, n, pos, total;
+};
+
+__host__ __device__ constexpr WarpLayout warp_layout(int M) {
+  WarpLayout w{};
+  w.rows = 0;
+  w.L = 512 * M * M;
+  w.P = w.L + 4 * 64 * M;
+  w.E = w.P + 4 * (64 * M + 1);
+  w.range = (w.E + 4 * (64 * M + 1) + 7) / 8 * 8;
+  w.don = w.range + 8;
+  w.busy = w.don + 4;
+  w.hn = w.busy + 4;
+  w.heavy = w.hn + 4;  // 32 deferred heavy items
+  w.ptr = (w.heavy + 4 * 32 + 7) / 8 * 8;
+  w.n = w.ptr + 8 * 16;
+  w.pos = w.n + 4 * 16;
+  w.total = (w.pos + 4 * 16 + 15) / 16 * 16;
+  return w;
 }
+
+struct CliqueArgs {
+  GraphView g;
+  const int32_t* roots;
+  int n_roots;
+  LBArgs lb;
+  int32_t* arena;               // list path: K * arena_dcap ints per warp
+  int arena_dcap;
+  int list_threshold;           // roots with d > list_threshold take the list path
+  unsigned long long* per_root; // optional: k-cliques found under each root (subtree logger)
+};
 
 // Loads L = N+(root) into shared memory and the exclusive prefix sum of the out-degrees
 // of its members (sP[0..d]). Returns the total.
@@ -124,360 +152,402 @@ __device__ __forceinline__ int load_root_list(const GraphView& g, int root, int 
   return carry;
 }
 
+// Local adjacency bitmap of L (rows zeroed by the caller): the (member, out-neighbour)
+// pairs are flattened so the warp stays busy when rows are short; membership in L is a
+// binary search in shared memory.
+__device__ __forceinline__ void build_local_rows(const GraphView& g, const int32_t* sL, const int32_t* sP, int d,
+                                                 int total, uint32_t* rows, int row_words) {
+  const int lane = lane_id();
+  const int32_t maxL = sL[d - 1];
+  for (int f = lane; f < total; f += 32) {
+    const int i = lower_bound(sP, 0, d + 1, f + 1) - 1;  // largest i with sP[i] <= f
+    const int32_t x = __ldg(g.adj + __ldg(g.row + sL[i]) + (f - sP[i]));
+    if (x <= maxL) {
+      const int j = lower_bound(sL, i + 1, d, x);
+      if (j < d && sL[j] == x) atomicOr(rows + i * row_words + (j >> 5), 1u << (j & 31));
+    }
+  }
+}
+
+constexpr int HEAVY_BITS = 24;  // an item whose candidate set has this many members is
+                                // run by the whole warp instead of one lane (k >= 6)
+constexpr int HEAVY_SLOTS = 32;
+
+// Counts the cliques of item `it` (a local edge c1 < c2, or a row c1 when k == 3) on one
+// lane. For k >= 6 an item with a large candidate set is deferred to the warp instead
+// (returns without counting) when a heavy slot is free.
 template <int K, int NW>
-__global__ void __launch_bounds__(256) clique_thread_kernel(GraphView g, const int32_t* __restrict__ tasks,
-                                                            int n_tasks, DevCounters* ctr, int slot) {
-  constexpr int DCAP = 64 * NW;
-  constexpr int RW = 2 * NW;
-  extern __shared__ __align__(16) unsigned char smem[];
-  const int lane = lane_id();
-  unsigned char* base = smem + thread_warp_smem<NW>() * warp_in_block();
-  uint32_t* rows = reinterpret_cast<uint32_t*>(base);
-  int32_t* sL = reinterpret_cast<int32_t*>(rows + DCAP * RW);
-  int32_t* sP = sL + DCAP;
-  int* sNext = sP + DCAP + 1;
-  unsigned long long cnt = 0, ntasks = 0;
-  while (true) {
-    int t = 0;
-    if (lane == 0) t = atomicAdd(&ctr->cursor[slot], 1);
-    t = __shfl_sync(FULL_MASK, t, 0);
-    if (t >= n_tasks) break;
-    ++ntasks;
-    const int root = __ldg(tasks + t);
-    const int d = __ldg(g.deg + root);
-    if constexpr (K == 2) {
-      if (lane == 0) cnt += (unsigned long long)d;
-      continue;
-    }
-    for (int i = lane; i < d * RW; i += 32) rows[i] = 0;
-    const int total = load_root_list(g, root, d, sL, sP);
-    if (lane == 0) *sNext = 32;
-    build_local_rows(g, sL, sP, d, total, rows, RW);
-    __syncwarp();
-    const uint64_t* rows64 = reinterpret_cast<const uint64_t*>(rows);
-    int c1 = lane;
-    while (c1 < d) {
-      Bits<NW> S;
+__device__ __forceinline__ unsigned long long bitmap_item(int it, const uint64_t* rows, const int32_t* sE, int d,
+                                                          int* hn, int* heavy) {
+  if constexpr (K == 3) {
+    Bits<NW> S;
 #pragma unroll
-      for (int j = 0; j < NW; ++j) S.w[j] = rows64[c1 * NW + j];
-      if (K == 3) cnt += (unsigned long long)popc(S);
-      else if (popc(S) >= K - 3) cnt += count_rec<(K >= 4 ? K - 3 : 0), NW>(S, rows64);
-      c1 = atomicAdd(sNext, 1);
-    }
-    __syncwarp();
-  }
-  cnt = warp_sum_u64(cnt);
-  if (lane == 0) {
-    atomicAdd(&ctr->count, cnt);
-    atomicAdd(&ctr->tasks, ntasks);
-  }
-}
-
-// ---------------- warp mode ----------------
-
-// Number of (D+1)-cliques inside a warp-distributed set (lane holds words lane, lane+32).
-template <int D>
-__device__ __forceinline__ unsigned long long wcount(uint32_t a, uint32_t b, const uint32_t* __restrict__ rows,
-                                                     int W) {
-  const int lane = lane_id();
-  if constexpr (D == 0) {
-    return (unsigned long long)(__popc(a) + __popc(b));
+    for (int w = 0; w < NW; ++w) S.w[w] = rows[it * NW + w];
+    return (unsigned long long)popc(S);
   } else {
-    unsigned long long sum = 0;
-    while (true) {
-      unsigned nz = __ballot_sync(FULL_MASK, a != 0);
-      int c;
-      if (nz) {
-        const int owner = __ffs(nz) - 1;
-        int bit = 0;
-        if (lane == owner) {
-          bit = __ffs(a) - 1;
-          a &= a - 1;
+    const int c1 = lower_bound(sE, 0, d + 1, it + 1) - 1;
+    const int c2 = select_bit<NW>(rows + c1 * NW, it - sE[c1]);
+    Bits<NW> S;
+#pragma unroll
+    for (int w = 0; w < NW; ++w) S.w[w] = rows[c1 * NW + w] & rows[c2 * NW + w];
+    if constexpr (K == 4) {
+      return (unsigned long long)popc(S);
+    } else {
+      const int p = popc(S);
+      if (p < K - 3) return 0;
+      if constexpr (K >= 6) {
+        if (p >= HEAVY_BITS && hn) {
+          const int slot = atomicAdd(hn, 1);
+          if (slot < HEAVY_SLOTS) {
+            heavy[slot] = it;
+            return 0;
+          }
         }
-        c = owner * 32 + __shfl_sync(FULL_MASK, bit, owner);
-      } else {
-        unsigned nz2 = __ballot_sync(FULL_MASK, b != 0);
-        if (!nz2) break;
-        const int owner = __ffs(nz2) - 1;
-        int bit = 0;
-        if (lane == owner) {
-          bit = __ffs(b) - 1;
-          b &= b - 1;
-        }
-        c = (owner + 32) * 32 + __shfl_sync(FULL_MASK, bit, owner);
       }
-      const uint32_t* rc = rows + (size_t)c * W;
-      const uint32_t ta = a & (lane < W ? __ldcg(rc + lane) : 0u);
-      const uint32_t tb = b & (lane + 32 < W ? __ldcg(rc + lane + 32) : 0u);
-      if constexpr (D == 1) {
-        sum += (unsigned long long)(__popc(ta) + __popc(tb));
-      } else {
-        if (__any_sync(FULL_MASK, (ta | tb) != 0)) sum += wcount<D - 1>(ta, tb, rows, W);
-      }
+      return count_rec<(K >= 5 ? K - 4 : 0), NW>(S, rows);
     }
-    return sum;
   }
 }
 
-constexpr int WARP_MODE_DMAX = 2048;
-constexpr int WARP_MODE_WARPS = 4;  // warps per block
-
-template <int K>
-__global__ void __launch_bounds__(32 * WARP_MODE_WARPS) clique_warp_kernel(GraphView g, const int32_t* __restrict__ tasks,
-                                                                          int n_tasks, DevCounters* ctr, int slot,
-                                                                          uint32_t* scratch, int dcap) {
-  extern __shared__ __align__(16) unsigned char smem[];
+// Warp-cooperative run of one heavy item: the third local vertex c3 is spread over the
+// lanes (the j-th member of the candidate set goes to lane j mod 32).
+template <int K, int NW>
+__device__ __forceinline__ unsigned long long heavy_item(int it, const uint64_t* rows, const int32_t* sE, int d) {
   const int lane = lane_id();
-  const int wib = warp_in_block();
-  int32_t* sL = reinterpret_cast<int32_t*>(smem) + (size_t)wib * (2 * WARP_MODE_DMAX + 4);
-  int32_t* sP = sL + WARP_MODE_DMAX;
-  const size_t gw = (size_t)blockIdx.x * WARP_MODE_WARPS + wib;
-  const int Wmax = (dcap + 31) / 32;
-  uint32_t* rows = scratch + gw * (size_t)dcap * Wmax;
-  unsigned long long cnt = 0, ntasks = 0;
-  while (true) {
-    int t = 0;
-    if (lane == 0) t = atomicAdd(&ctr->cursor[slot], 1);
-    t = __shfl_sync(FULL_MASK, t, 0);
-    if (t >= n_tasks) break;
-    ++ntasks;
-    const int root = __ldg(tasks + t);
-    const int d = __ldg(g.deg + root);
-    if (d > dcap || d > WARP_MODE_DMAX) {
-      if (lane == 0) atomicCAS(&ctr->err, 0, ERR_BAD_TASK);
-      continue;
+  const int c1 = lower_bound(sE, 0, d + 1, it + 1) - 1;
+  const int c2 = select_bit<NW>(rows + c1 * NW, it - sE[c1]);
+  Bits<NW> S;
+#pragma unroll
+  for (int w = 0; w < NW; ++w) S.w[w] = rows[c1 * NW + w] & rows[c2 * NW + w];
+  unsigned long long sum = 0;
+  int j = 0;
+#pragma unroll
+  for (int wi = 0; wi < NW; ++wi) {
+    uint64_t bits = S.w[wi];
+    while (bits) {
+      const int b = __ffsll((long long)bits) - 1;
+      bits &= bits - 1;
+      if ((j++ & 31) != lane) continue;
+      const uint64_t* rc = rows + (wi * 64 + b) * NW;
+      Bits<NW> T;
+#pragma unroll
+      for (int w = 0; w < NW; ++w) T.w[w] = (w < wi ? 0ull : (w == wi ? bits : S.w[w])) & rc[w];
+      if (popc(T) >= K - 4) sum += count_rec<(K >= 6 ? K - 5 : 0), NW>(T, rows);
     }
-    const int W = (d + 31) / 32;
-    for (int i = lane; i < d * W; i += 32) rows[i] = 0;
-    const int total = load_root_list(g, root, d, sL, sP);
-    __syncwarp();
-    __threadfence_block();
-    build_local_rows(g, sL, sP, d, total, rows, W);
-    __syncwarp();
-    __threadfence_block();
-    for (int c1 = 0; c1 < d; ++c1) {
-      const uint32_t* rc = rows + (size_t)c1 * W;
-      uint32_t a = lane < W ? __ldcg(rc + lane) : 0u;
-      uint32_t b = lane + 32 < W ? __ldcg(rc + lane + 32) : 0u;
-      if (K == 3) cnt += (unsigned long long)(__popc(a) + __popc(b));
-      else if (__any_sync(FULL_MASK, (a | b) != 0)) cnt += wcount<(K >= 4 ? K - 3 : 0)>(a, b, rows, W);
-    }
-    __syncwarp();
   }
-  cnt = warp_sum_u64(cnt);
+  return sum;
+}
+
+// Bitmap path for one task. Returns the k-cliques counted by this lane.
+template <int K, int NW, int M>
+__device__ unsigned long long bitmap_task(const CliqueArgs& a, unsigned char* wsm, int root, int d, int b, int e) {
+  constexpr WarpLayout LY = warp_layout(M);
+  constexpr int RW = 2 * NW;
+  const int lane = lane_id();
+  uint32_t* rows32 = reinterpret_cast<uint32_t*>(wsm + LY.rows);
+  int32_t* sL = reinterpret_cast<int32_t*>(wsm + LY.L);
+  int32_t* sP = reinterpret_cast<int32_t*>(wsm + LY.P);
+  int32_t* sE = reinterpret_cast<int32_t*>(wsm + LY.E);
+  unsigned long long* range = reinterpret_cast<unsigned long long*>(wsm + LY.range);
+  int* donations_left = reinterpret_cast<int*>(wsm + LY.don);
+  int* busy = reinterpret_cast<int*>(wsm + LY.busy);
+  int* hn = reinterpret_cast<int*>(wsm + LY.hn);
+  int* heavy = reinterpret_cast<int*>(wsm + LY.heavy);
+  const long long t_start = global_ns();
+  for (int i = lane; i < d * RW; i += 32) rows32[i] = 0;
+  const int total = load_root_list(a.g, root, d, sL, sP);
+  build_local_rows(a.g, sL, sP, d, total, rows32, RW);
+  __syncwarp();
+  const uint64_t* rows = reinterpret_cast<const uint64_t*>(rows32);
+  int n_items;
+  if constexpr (K >= 4) {
+    // exclusive prefix of row popcounts: the items are the local edges
+    int carry = 0;
+    for (int i0 = 0; i0 < d; i0 += 32) {
+      const int i = i0 + lane;
+      int pc = 0;
+      if (i < d) {
+#pragma unroll
+        for (int w = 0; w < NW; ++w) pc += __popcll(rows[i * NW + w]);
+      }
+      int s = pc;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        int y = __shfl_up_sync(FULL_MASK, s, o);
+        if (lane >= o) s += y;
+      }
+      if (i < d) sE[i] = carry + s - pc;
+      carry += __shfl_sync(FULL_MASK, s, 31);
+    }
+    if (lane == 0) sE[d] = carry;
+    n_items = carry;
+  } else {
+    n_items = d;
+  }
+  const int hi = e < 0 ? n_items : min(e, n_items);
   if (lane == 0) {
-    atomicAdd(&ctr->count, cnt);
-    atomicAdd(&ctr->tasks, ntasks);
+    *range = pack_range(b, hi);
+    *donations_left = a.lb.max_donations;
+    *busy = 0;
+    *hn = 0;
   }
-}
-
-// ---------------- list mode ----------------
-
-constexpr int LIST_WARPS = 8;
-
-template <int K>
-__global__ void __launch_bounds__(32 * LIST_WARPS) clique_list_kernel(GraphView g, const int32_t* __restrict__ tasks,
-                                                                     int n_tasks, DevCounters* ctr, int slot,
-                                                                     int32_t* arena, int dcap) {
-  __shared__ const int32_t* sPtr[LIST_WARPS][K];
-  __shared__ int sN[LIST_WARPS][K];
-  __shared__ int sPos[LIST_WARPS][K];
-  const int lane = lane_id();
-  const int wib = warp_in_block();
-  const size_t gw = (size_t)blockIdx.x * LIST_WARPS + wib;
-  int32_t* my = arena + gw * (size_t)K * dcap;
-  unsigned long long cnt = 0, ntasks = 0, nodes = 0;
+  __syncwarp();
+  unsigned long long cnt = 0;
+  unsigned done = 0;
   while (true) {
-    int t = 0;
-    if (lane == 0) t = atomicAdd(&ctr->cursor[slot], 1);
-    t = __shfl_sync(FULL_MASK, t, 0);
-    if (t >= n_tasks) break;
-    ++ntasks;
-    const int root = __ldg(tasks + t);
-    const int d = __ldg(g.deg + root);
-    if (K == 2) {
-      if (lane == 0) cnt += (unsigned long long)d;
-      continue;
+    const int it = range_take(range);
+    if (it < 0) break;
+    cnt += bitmap_item<K, NW>(it, rows, sE, d, hn, heavy);
+    if ((++done & 15) == 0) {
+      int ob = 0, oe = 0;
+      if (range_maybe_donate(a.lb, range, root, donations_left, t_start, busy, ob, oe)) {
+        for (int j = ob; j < oe; ++j) cnt += bitmap_item<K, NW>(j, rows, sE, d, nullptr, nullptr);
+      }
+      if ((done & 255) == 0) atomicAdd(&a.lb.ctr->progress, 256ull);
     }
-    if (d > dcap) {
-      if (lane == 0) atomicCAS(&ctr->err, 0, ERR_ARENA_OVERFLOW);
-      continue;
-    }
-    if (lane == 0) {
-      sPtr[wib][0] = g.adj + g.row[root];
-      sN[wib][0] = d;
-      sPos[wib][0] = 0;
+  }
+  __syncwarp();
+  if constexpr (K >= 6) {
+    const int nh = min(*hn, HEAVY_SLOTS);
+    for (int h = 0; h < nh; ++h) {
+      cnt += heavy_item<K, NW>(heavy[h], rows, sE, d);
+      if (lane == 0) atomicAdd(&a.lb.ctr->progress, 1ull);
     }
     __syncwarp();
-    int lvl = 0;
-    while (lvl >= 0) {
-      const int pos = sPos[wib][lvl];
-      const int rem = sN[wib][lvl] - pos;
-      if (rem - 1 < K - 2 - lvl) {
-        --lvl;
-        continue;
+  }
+  return cnt;
+}
+
+// List path for one task (warp-cooperative). Returns this lane's share of the count.
+template <int K, int M>
+__device__ unsigned long long list_task(const CliqueArgs& a, unsigned char* wsm, int root, int d, int b, int e,
+                                        int32_t* my_arena) {
+  constexpr WarpLayout LY = warp_layout(M);
+  const int lane = lane_id();
+  unsigned long long* range = reinterpret_cast<unsigned long long*>(wsm + LY.range);
+  int* donations_left = reinterpret_cast<int*>(wsm + LY.don);
+  int* busy = reinterpret_cast<int*>(wsm + LY.busy);
+  const long long t_start = global_ns();
+  const int32_t** sPtr = reinterpret_cast<const int32_t**>(wsm + LY.ptr);
+  int* sN = reinterpret_cast<int*>(wsm + LY.n);
+  int* sPos = reinterpret_cast<int*>(wsm + LY.pos);
+  const int32_t* L = a.g.adj + __ldg(a.g.row + root);
+  const int hi = e < 0 ? d : min(e, d);
+  if (lane == 0) {
+    *range = pack_range(b, hi);
+    *donations_left = a.lb.max_donations;
+    *busy = 0;
+  }
+  __syncwarp();
+  unsigned long long cnt = 0;
+  while (true) {
+    int it = 0;
+    if (lane == 0) {
+      it = range_take(range);
+      int ob = 0, oe = 0;
+      if (it >= 0 && range_maybe_donate(a.lb, range, root, donations_left, t_start, busy, ob, oe)) {
+        // lane 0 is the only taker here, so the split can be undone
+        const unsigned long long cur = *reinterpret_cast<volatile unsigned long long*>(range);
+        *range = (cur & 0xffffffffull) | ((unsigned long long)(unsigned)oe << 32);
       }
-      const int32_t* P = sPtr[wib][lvl];
-      const int c = P[pos];
+    }
+    it = __shfl_sync(FULL_MASK, it, 0);
+    if (it < 0) break;
+    const int c = __ldg(L + it);
+    const int32_t* A = L + it + 1;
+    const int na = d - it - 1;
+    if (na < K - 2) continue;
+    const int32_t* B = a.g.adj + __ldg(a.g.row + c);
+    const int nb = __ldg(a.g.deg + c);
+    if constexpr (K == 3) {
+      unsigned s = 0;
+      for (int i = lane; i < na; i += 32) s += contains(B, nb, __ldg(A + i)) ? 1u : 0u;
+      cnt += s;
+    } else {
+      // C1 = A cap N+(c), written to level 1 of the arena
+      int32_t* out1 = my_arena + a.arena_dcap;
+      int m = 0;
+      for (int i0 = 0; i0 < na; i0 += 32) {
+        const int i = i0 + lane;
+        const int32_t x = i < na ? __ldg(A + i) : 0;
+        m += compact(out1, m, x, i < na && contains(B, nb, x));
+      }
       __syncwarp();
-      if (lane == 0) sPos[wib][lvl] = pos + 1;
-      // extend: candidates after c intersected with N+(c)
-      const int32_t* A = P + pos + 1;
-      const int na = rem - 1;
-      const int32_t* B = g.adj + __ldg(g.row + c);
-      const int nb = __ldg(g.deg + c);
-      ++nodes;
-      if (lvl + 1 == K - 2) {
-        unsigned s = 0;
-        for (int i = lane; i < na; i += 32) s += contains(B, nb, A[i]) ? 1u : 0u;
-        cnt += s;
-      } else {
-        int32_t* out = my + (size_t)(lvl + 1) * dcap;
-        int m = 0;
-        for (int i0 = 0; i0 < na; i0 += 32) {
-          const int i = i0 + lane;
-          const int32_t x = i < na ? A[i] : 0;
-          const bool ok = i < na && contains(B, nb, x);
-          m += compact(out, m, x, ok);
+      if (lane == 0) {
+        sPtr[1] = out1;
+        sN[1] = m;
+        sPos[1] = 0;
+      }
+      __syncwarp();
+      int lvl = 1;
+      while (lvl >= 1) {
+        const int pos = sPos[lvl];
+        const int rem = sN[lvl] - pos;
+        if (rem - 1 < K - 2 - lvl) {
+          --lvl;
+          continue;
+        }
+        const int32_t* P = sPtr[lvl];
+        const int v = P[pos];
+        __syncwarp();
+        if (lane == 0) {
+          sPos[lvl] = pos + 1;
+          if ((pos & 63) == 63) atomicAdd(&a.lb.ctr->progress, 64ull);
+        }
+        const int32_t* A2 = P + pos + 1;
+        const int na2 = rem - 1;
+        const int32_t* B2 = a.g.adj + __ldg(a.g.row + v);
+        const int nb2 = __ldg(a.g.deg + v);
+        if (lvl + 1 == K - 2) {
+          unsigned s = 0;
+          for (int i = lane; i < na2; i += 32) s += contains(B2, nb2, A2[i]) ? 1u : 0u;
+          cnt += s;
+        } else {
+          int32_t* out = my_arena + (size_t)(lvl + 1) * a.arena_dcap;
+          int m2 = 0;
+          for (int i0 = 0; i0 < na2; i0 += 32) {
+            const int i = i0 + lane;
+            const int32_t x = i < na2 ? A2[i] : 0;
+            m2 += compact(out, m2, x, i < na2 && contains(B2, nb2, x));
+          }
+          __syncwarp();
+          ++lvl;
+          if (lane == 0) {
+            sPtr[lvl] = out;
+            sN[lvl] = m2;
+            sPos[lvl] = 0;
+          }
         }
         __syncwarp();
-        ++lvl;
-        if (lane == 0) {
-          sPtr[wib][lvl] = out;
-          sN[wib][lvl] = m;
-          sPos[wib][lvl] = 0;
+      }
+    }
+  }
+  __syncwarp();
+  return cnt;
+}
+
+template <int K, int M>
+__global__ void __launch_bounds__(256) clique_kernel(CliqueArgs a) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  constexpr WarpLayout LY = warp_layout(M);
+  const int lane = lane_id();
+  unsigned char* wsm = smem + (size_t)LY.total * warp_in_block();
+  const size_t gw = (size_t)blockIdx.x * (blockDim.x >> 5) + warp_in_block();
+  const int total_warps = gridDim.x * (blockDim.x >> 5);
+  int32_t* my_arena = a.arena ? a.arena + gw * (size_t)K * a.arena_dcap : nullptr;
+  unsigned long long cnt = 0, ntasks = 0;
+  while (true) {
+    int first = 0, count = 0, b = 0, e = -1, ok = 0;
+    bool donated = false;
+    if (lane == 0) ok = lb_next(a.lb, a.n_roots, total_warps, first, count, b, e, donated) ? 1 : 0;
+    ok = __shfl_sync(FULL_MASK, ok, 0);
+    if (!ok) break;
+    first = __shfl_sync(FULL_MASK, first, 0);
+    count = __shfl_sync(FULL_MASK, count, 0);
+    b = __shfl_sync(FULL_MASK, b, 0);
+    e = __shfl_sync(FULL_MASK, e, 0);
+    donated = __shfl_sync(FULL_MASK, donated ? 1 : 0, 0) != 0;
+    for (int ti = 0; ti < count; ++ti) {
+      const int root = donated ? first : __ldg(a.roots + first + ti);
+      ++ntasks;
+      unsigned long long task_cnt = 0;
+      const int d = __ldg(a.g.deg + root);
+      if (e >= 0 && b >= e) {
+        // empty donation: nothing to do
+      } else if (K == 2) {
+        if (lane == 0) task_cnt = (unsigned long long)d;
+      } else if (d > a.list_threshold) {
+        if (K > 3 && (!my_arena || d > a.arena_dcap)) {
+          if (lane == 0) set_err(a.lb.ctr, ERR_ARENA_OVERFLOW);
+        } else {
+          task_cnt = list_task<K, M>(a, wsm, root, d, b, e, my_arena);
         }
+      } else {
+        const int nw = (d + 63) >> 6;
+        if (nw <= 1) task_cnt = bitmap_task<K, 1, M>(a, wsm, root, d, b, e);
+        else if (M >= 2 && nw == 2) task_cnt = bitmap_task<K, (M >= 2 ? 2 : 1), M>(a, wsm, root, d, b, e);
+        else if (M >= 3 && nw == 3) task_cnt = bitmap_task<K, (M >= 3 ? 3 : 1), M>(a, wsm, root, d, b, e);
+        else if (M >= 4 && nw == 4) task_cnt = bitmap_task<K, (M >= 4 ? 4 : 1), M>(a, wsm, root, d, b, e);
+        else if (lane == 0) set_err(a.lb.ctr, ERR_BAD_TASK);
+      }
+      cnt += task_cnt;
+      if (a.per_root) {
+        const unsigned long long tsum = warp_sum_u64(task_cnt);
+        if (lane == 0 && tsum) atomicAdd(a.per_root + root, tsum);
       }
       __syncwarp();
     }
+    if (lane == 0) lb_done(a.lb, count);
   }
   cnt = warp_sum_u64(cnt);
   if (lane == 0) {
-    atomicAdd(&ctr->count, cnt);
-    atomicAdd(&ctr->tasks, ntasks);
-    atomicAdd(&ctr->nodes, nodes);
+    atomicAdd(&a.lb.ctr->count, cnt);
+    atomicAdd(&a.lb.ctr->tasks, ntasks);
   }
 }
 
-// ---------------- host launchers ----------------
+// ---------------- host launcher ----------------
 
-template <typename Kern>
-static int grid_for(Kern kern, int block, size_t smem, const LaunchCtx& ctx, int* grid) {
-  int occ = 0;
-  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, block, smem);
-  if (e != cudaSuccess) return fail(DM_ECUDA, std::string("occupancy query failed: ") + cudaGetErrorString(e));
-  if (occ < 1) return fail(DM_EINVAL, "kernel does not fit on an SM with the requested block size");
-  *grid = ctx.num_sms * occ;
-  if (ctx.threads > 0 && ctx.block > 0) {
-    // the reference's (threads, blockSize) pair maps onto the persistent grid
-    int want = (ctx.threads + block - 1) / block;
-    *grid = want < 1 ? 1 : want;
-  }
-  return DM_OK;
-}
+constexpr int CLIQUE_BLOCK = 256;
 
-template <int K, int NW>
-static int launch_thread(const GraphView& g, const int32_t* tasks, int n, DevCounters* ctr, int slot, LaunchCtx& ctx) {
-  if (n == 0) return DM_OK;
-  const int block = 256;
-  const size_t smem = thread_warp_smem<NW>() * (block / 32);
-  auto kern = clique_thread_kernel<K, NW>;
-  if (smem > 48 * 1024) DM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  int grid = 0;
-  int rc = grid_for(kern, block, smem, ctx, &grid);
-  if (rc) return rc;
-  kern<<<grid, block, smem, ctx.stream>>>(g, tasks, n, ctr, slot);
-  ctx.launches++;
-  DM_CUDA(cudaGetLastError());
-  return DM_OK;
-}
-
-template <int K>
-static int launch_warp(const GraphView& g, const int32_t* tasks, int n, DevCounters* ctr, int slot, LaunchCtx& ctx,
-                       void* scratch, size_t bytes, int dcap) {
-  if (n == 0) return DM_OK;
-  const int block = 32 * WARP_MODE_WARPS;
-  auto kern = clique_warp_kernel<K>;
-  const size_t smem = sizeof(int32_t) * (2 * WARP_MODE_DMAX + 4) * WARP_MODE_WARPS;
+template <int K, int M>
+static int launch_k(const CliqueArgs& a, LaunchCtx& ctx, int* grid_out) {
+  const size_t smem = (size_t)warp_layout(M).total * (CLIQUE_BLOCK / 32);
+  auto kern = clique_kernel<K, M>;
   DM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  int grid = 0;
-  int rc = grid_for(kern, block, smem, ctx, &grid);
-  if (rc) return rc;
-  const size_t per_warp = (size_t)dcap * ((dcap + 31) / 32) * sizeof(uint32_t);
-  const size_t max_warps = bytes / per_warp;
-  if ((size_t)grid * WARP_MODE_WARPS > max_warps) grid = (int)(max_warps / WARP_MODE_WARPS);
-  if (grid < 1) return fail(DM_ENOMEM, "warp-mode scratch too small");
-  kern<<<grid, block, smem, ctx.stream>>>(g, tasks, n, ctr, slot, reinterpret_cast<uint32_t*>(scratch), dcap);
+  int occ = 0;
+  DM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, CLIQUE_BLOCK, smem));
+  if (occ < 1) return fail(DM_EINVAL, "clique kernel does not fit on an SM");
+  int grid = ctx.num_sms * occ;
+  if (ctx.threads > 0) grid = std::max(1, std::min(grid, (ctx.threads + CLIQUE_BLOCK - 1) / CLIQUE_BLOCK));
+  if (a.arena && grid * (CLIQUE_BLOCK / 32) > ctx.arena_warps) grid = std::max(1, ctx.arena_warps / (CLIQUE_BLOCK / 32));
+  CliqueArgs args = a;
+  const int warps = grid * (CLIQUE_BLOCK / 32);
+  args.lb.hungry_trigger =
+      ctx.threshold >= 100 ? 0 : std::max(1, (ctx.threshold * warps + 99) / 100);
+  kern<<<grid, CLIQUE_BLOCK, smem, ctx.stream>>>(args);
   ctx.launches++;
+  *grid_out = grid;
   DM_CUDA(cudaGetLastError());
   return DM_OK;
 }
 
 template <int K>
-static int launch_list(const GraphView& g, const int32_t* tasks, int n, DevCounters* ctr, int slot, LaunchCtx& ctx,
-                       void* scratch, size_t bytes, int dcap) {
-  if (n == 0) return DM_OK;
-  const int block = 32 * LIST_WARPS;
-  auto kern = clique_list_kernel<K>;
-  int grid = 0;
-  int rc = grid_for(kern, block, 0, ctx, &grid);
-  if (rc) return rc;
-  const size_t per_warp = (size_t)K * dcap * sizeof(int32_t);
-  const size_t max_warps = bytes / per_warp;
-  if ((size_t)grid * LIST_WARPS > max_warps) grid = (int)(max_warps / LIST_WARPS);
-  if (grid < 1) return fail(DM_ENOMEM, "list-mode arena too small");
-  kern<<<grid, block, 0, ctx.stream>>>(g, tasks, n, ctr, slot, reinterpret_cast<int32_t*>(scratch), dcap);
-  ctx.launches++;
-  DM_CUDA(cudaGetLastError());
-  return DM_OK;
+static int launch_nw(const CliqueArgs& a, int m, LaunchCtx& ctx, int* grid) {
+  switch (m) {
+    case 1: return launch_k<K, 1>(a, ctx, grid);
+    case 2: return launch_k<K, 2>(a, ctx, grid);
+    case 3: return launch_k<K, 3>(a, ctx, grid);
+    default: return launch_k<K, 4>(a, ctx, grid);
+  }
 }
 
-static size_t list_bytes(const CliqueTasks& t, int k, const LaunchCtx& ctx) {
-  if (!t.n_list) return 0;
-  size_t warps = (size_t)ctx.num_sms * 8 * LIST_WARPS;
-  return warps * (size_t)k * (t.max_list_deg + 4) * sizeof(int32_t);
-}
+int clique_max_warps(int num_sms) { return num_sms * 64; }
 
-static size_t warp_bytes(const CliqueTasks& t, const LaunchCtx& ctx) {
-  if (!t.n_warp) return 0;
-  const int dcap = t.max_warp_deg;
-  size_t per_warp = (size_t)dcap * ((dcap + 31) / 32) * sizeof(uint32_t);
-  size_t warps = (size_t)ctx.num_sms * 4 * WARP_MODE_WARPS;
-  return warps * per_warp;
-}
-
-size_t clique_scratch_bytes(const CliqueTasks& t, int k, const LaunchCtx& ctx) {
-  size_t a = list_bytes(t, k, ctx), b = warp_bytes(t, ctx);
-  return a > b ? a : b;
-}
-
-template <int K>
-static int run_k(const GraphView& g, const CliqueTasks& t, DevCounters* ctr, LaunchCtx& ctx, void* scratch,
-                 size_t bytes) {
-  int rc = DM_OK;
-  // heaviest first: list roots, warp-mode roots, then the bulk in thread mode
-  if (!rc) rc = launch_list<K>(g, t.d_list, t.n_list, ctr, 0, ctx, scratch, bytes, t.max_list_deg + 4);
-  if (!rc) rc = launch_warp<K>(g, t.d_warp, t.n_warp, ctr, 1, ctx, scratch, bytes, t.max_warp_deg);
-  if (!rc) rc = launch_thread<K, 2>(g, t.d_thread2, t.n_thread2, ctr, 2, ctx);
-  if (!rc) rc = launch_thread<K, 1>(g, t.d_thread1, t.n_thread1, ctr, 3, ctx);
-  return rc;
-}
-
-int clique_launch(const GraphView& g, int k, const CliqueTasks& t, DevCounters* ctr, LaunchCtx& ctx, void* scratch,
-                  size_t bytes, dm_stats* st) {
-  (void)st;
-  switch (k) {
-    case 2: return run_k<2>(g, t, ctr, ctx, scratch, bytes);
-    case 3: return run_k<3>(g, t, ctr, ctx, scratch, bytes);
-    case 4: return run_k<4>(g, t, ctr, ctx, scratch, bytes);
-    case 5: return run_k<5>(g, t, ctr, ctx, scratch, bytes);
-    case 6: return run_k<6>(g, t, ctr, ctx, scratch, bytes);
-    case 7: return run_k<7>(g, t, ctr, ctx, scratch, bytes);
-    case 8: return run_k<8>(g, t, ctr, ctx, scratch, bytes);
-    case 9: return run_k<9>(g, t, ctr, ctx, scratch, bytes);
-    case 10: return run_k<10>(g, t, ctr, ctx, scratch, bytes);
-    case 11: return run_k<11>(g, t, ctr, ctx, scratch, bytes);
-    case 12: return run_k<12>(g, t, ctr, ctx, scratch, bytes);
+int clique_launch(const CliqueLaunch& L, LaunchCtx& ctx, int* grid) {
+  CliqueArgs a;
+  a.g = L.g;
+  a.roots = L.roots;
+  a.n_roots = L.n_roots;
+  a.lb = LBArgs{L.ctr, reinterpret_cast<QHeader*>(L.queue),
+                reinterpret_cast<QSlot*>(reinterpret_cast<char*>(L.queue) + sizeof(QHeader)), L.qcap, 0,
+                L.max_donations, (long long)ctx.donate_after_us * 1000ll, (long long)ctx.timeout_ms * 1000000ll};
+  a.arena = L.arena;
+  a.arena_dcap = L.arena_dcap;
+  a.list_threshold = L.list_threshold;
+  a.per_root = L.per_root;
+  switch (L.k) {
+    case 2: return launch_nw<2>(a, L.nwmax, ctx, grid);
+    case 3: return launch_nw<3>(a, L.nwmax, ctx, grid);
+    case 4: return launch_nw<4>(a, L.nwmax, ctx, grid);
+    case 5: return launch_nw<5>(a, L.nwmax, ctx, grid);
+    case 6: return launch_nw<6>(a, L.nwmax, ctx, grid);
+    case 7: return launch_nw<7>(a, L.nwmax, ctx, grid);
+    case 8: return launch_nw<8>(a, L.nwmax, ctx, grid);
+    case 9: return launch_nw<9>(a, L.nwmax, ctx, grid);
+    case 10: return launch_nw<10>(a, L.nwmax, ctx, grid);
+    case 11: return launch_nw<11>(a, L.nwmax, ctx, grid);
+    case 12: return launch_nw<12>(a, L.nwmax, ctx, grid);
     default: return fail(DM_EINVAL, "k must be in [2, 12]");
   }
 }

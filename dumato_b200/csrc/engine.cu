@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "engine.hpp"
+#include "lb.cuh"
 
 namespace dmb {
 
@@ -35,8 +36,34 @@ struct Workspace {
   int32_t* d_q2c = nullptr;
   size_t q2c_cap = 0;
   const void* q2c_owner = nullptr;  // dictionary whose table is resident
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  void* d_queue = nullptr;          // donation queue, ready flags kept zero between calls
+  int qcap = 0;
+  unsigned long long* d_per_root = nullptr;
+  size_t per_root_cap = 0;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr, k0 = nullptr, k1 = nullptr;
 };
+
+constexpr int QUEUE_SLOTS = 1 << 16;
+
+__global__ void queue_init_kernel(QHeader* h, QSlot* q, int cap) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i == 0) {
+    h->write_pos = 0;
+    h->read_pos = 0;
+  }
+  if (i < cap) {
+    q[i].seq = (unsigned)i;
+    q[i].root = q[i].begin = q[i].end = 0;
+  }
+}
+
+static int init_queue(Workspace& ws, cudaStream_t st) {
+  QHeader* h = reinterpret_cast<QHeader*>(ws.d_queue);
+  QSlot* q = reinterpret_cast<QSlot*>(reinterpret_cast<char*>(ws.d_queue) + sizeof(QHeader));
+  queue_init_kernel<<<(ws.qcap + 255) / 256, 256, 0, st>>>(h, q, ws.qcap);
+  DM_CUDA(cudaGetLastError());
+  return DM_OK;
+}
 
 struct DeviceSlot {
   DeviceGraph dg;
@@ -77,11 +104,11 @@ static int select_device(const dm_opts* o, LaunchCtx& ctx) {
     ctx.stream = g_streams[dev];
   }
   if (o) {
-    ctx.timeout_ms = o->timeout_ms > 0 ? o->timeout_ms : 2000;
+    ctx.timeout_ms = o->timeout_ms > 0 ? o->timeout_ms : 30000;
     ctx.threads = o->threads;
     ctx.block = o->block_size;
     ctx.vwarp = o->vwarp;
-    ctx.threshold = o->threshold > 0 ? o->threshold : 100;
+    ctx.threshold = o->threshold > 0 ? o->threshold : 0;
     ctx.donations_per_warp = o->donations_per_warp > 0 ? o->donations_per_warp : 16;
   }
   return DM_OK;
@@ -133,12 +160,35 @@ static int ensure_ws_bytes(void** p, size_t* cap, size_t want) {
   return DM_OK;
 }
 
-static int prepare_ws(Workspace& ws) {
+static int prepare_ws(Workspace& ws, cudaStream_t st) {
   if (!ws.d_ctr) DM_CUDA(cudaMalloc(&ws.d_ctr, sizeof(DevCounters)));
   if (!ws.ev0) {
     DM_CUDA(cudaEventCreate(&ws.ev0));
     DM_CUDA(cudaEventCreate(&ws.ev1));
+    DM_CUDA(cudaEventCreate(&ws.k0));
+    DM_CUDA(cudaEventCreate(&ws.k1));
   }
+  if (!ws.d_queue) {
+    DM_CUDA(cudaMalloc(&ws.d_queue, sizeof(QHeader) + QUEUE_SLOTS * sizeof(QSlot)));
+    ws.qcap = QUEUE_SLOTS;
+    int rc = init_queue(ws, st);
+    if (rc) return rc;
+  }
+  return DM_OK;
+}
+
+// Initial counters: every root task is pending until a warp finishes it.
+static int init_counters(Workspace& ws, int n_roots, cudaStream_t st) {
+  DevCounters h;
+  std::memset(&h, 0, sizeof(h));
+  h.pending = n_roots;
+  DM_CUDA(cudaMemcpyAsync(ws.d_ctr, &h, sizeof(h), cudaMemcpyHostToDevice, st));
+  return DM_OK;
+}
+
+// A call that ended in an error may leave tasks in the queue: start the next one clean.
+static int reset_queue(Workspace& ws, const DevCounters& h, cudaStream_t st) {
+  if (h.err) return init_queue(ws, st);
   return DM_OK;
 }
 
@@ -159,8 +209,12 @@ void release_device_graphs(dm_graph* g) {
       cudaFree(s->ws.d_scratch);
       cudaFree(s->ws.d_hist);
       cudaFree(s->ws.d_q2c);
+      cudaFree(s->ws.d_queue);
+      cudaFree(s->ws.d_per_root);
       if (s->ws.ev0) cudaEventDestroy(s->ws.ev0);
       if (s->ws.ev1) cudaEventDestroy(s->ws.ev1);
+      if (s->ws.k0) cudaEventDestroy(s->ws.k0);
+      if (s->ws.k1) cudaEventDestroy(s->ws.k1);
       cudaSetDevice(cur);
     }
     cudaGetLastError();
@@ -250,14 +304,14 @@ int dm_count_cliques(dm_graph* g, int32_t k, const dm_opts* o, uint64_t* count, 
   ensure_oriented(g);
   DeviceSlot* s = slot_for(g, ctx.device);
   Workspace& ws = s->ws;
-  if ((rc = prepare_ws(ws))) return rc;
+  if ((rc = prepare_ws(ws, ctx.stream))) return rc;
   DM_CUDA(cudaEventRecord(ws.ev0, ctx.stream));
   if (!s->dg.has_oriented) {
     rc = upload_csr(g->orow, g->oadj, g->n, &s->dg.d_orow, &s->dg.d_odeg, &s->dg.d_oadj, ctx.stream);
     if (rc) return rc;
     s->dg.has_oriented = true;
   }
-  // tasks: roots with at least k-1 out-neighbours
+  // tasks: roots (rank space) with at least k-1 out-neighbours
   const int need = k - 1;
   std::vector<int32_t> roots;
   roots.reserve(g->n);
@@ -265,69 +319,73 @@ int dm_count_cliques(dm_graph* g, int32_t k, const dm_opts* o, uint64_t* count, 
     if (g->orow[r + 1] - g->orow[r] >= need) roots.push_back(r);
   if ((rc = order_roots(g, o, k, true, roots))) return rc;
   const int mode = o ? o->mode : DM_MODE_AUTO;
-  std::vector<int32_t> t1, t2, tw, tl;
-  int max_w = 0, max_l = 0;
-  for (int32_t r : roots) {
-    const int d = (int)(g->orow[r + 1] - g->orow[r]);
-    if (mode == DM_MODE_LIST || d > 2048) {
-      tl.push_back(r);
-      max_l = std::max(max_l, d);
-    } else if (d > 128) {
-      tw.push_back(r);
-      max_w = std::max(max_w, d);
-    } else if (d > 64) {
-      t2.push_back(r);
-    } else {
-      t1.push_back(r);
-    }
+  int max_d = 0;
+  for (int32_t r : roots) max_d = std::max(max_d, (int)(g->orow[r + 1] - g->orow[r]));
+  CliqueLaunch L;
+  L.k = k;
+  if (mode == DM_MODE_LIST) {
+    L.nwmax = 1;
+    L.list_threshold = -1;
+  } else {
+    L.nwmax = std::min(4, std::max(1, (std::min(max_d, 256) + 63) / 64));
+    L.list_threshold = 64 * L.nwmax;
   }
-  std::vector<int32_t> all;
-  all.reserve(roots.size());
-  all.insert(all.end(), tl.begin(), tl.end());
-  all.insert(all.end(), tw.begin(), tw.end());
-  all.insert(all.end(), t2.begin(), t2.end());
-  all.insert(all.end(), t1.begin(), t1.end());
-  if ((rc = ensure_ws_bytes(reinterpret_cast<void**>(&ws.d_tasks), &ws.tasks_cap, sizeof(int32_t) * (all.size() + 1))))
+  const bool need_arena = max_d > L.list_threshold && k > 3;
+  if ((rc = ensure_ws_bytes(reinterpret_cast<void**>(&ws.d_tasks), &ws.tasks_cap, sizeof(int32_t) * (roots.size() + 1))))
     return rc;
-  if (!all.empty())
-    DM_CUDA(cudaMemcpyAsync(ws.d_tasks, all.data(), sizeof(int32_t) * all.size(), cudaMemcpyHostToDevice, ctx.stream));
-  CliqueTasks t;
-  t.d_list = ws.d_tasks;
-  t.n_list = (int)tl.size();
-  t.d_warp = t.d_list + t.n_list;
-  t.n_warp = (int)tw.size();
-  t.d_thread2 = t.d_warp + t.n_warp;
-  t.n_thread2 = (int)t2.size();
-  t.d_thread1 = t.d_thread2 + t.n_thread2;
-  t.n_thread1 = (int)t1.size();
-  t.max_warp_deg = max_w;
-  t.max_list_deg = max_l;
-  const size_t sb = clique_scratch_bytes(t, k, ctx);
-  if (sb && (rc = ensure_ws_bytes(&ws.d_scratch, &ws.scratch_cap, sb))) return rc;
-  DM_CUDA(cudaMemsetAsync(ws.d_ctr, 0, sizeof(DevCounters), ctx.stream));
-  cudaEvent_t k0, k1;
-  DM_CUDA(cudaEventCreate(&k0));
-  DM_CUDA(cudaEventCreate(&k1));
-  DM_CUDA(cudaEventRecord(k0, ctx.stream));
-  GraphView view{s->dg.d_orow, s->dg.d_odeg, s->dg.d_oadj, g->n};
-  rc = clique_launch(view, k, t, ws.d_ctr, ctx, ws.d_scratch, ws.scratch_cap, st);
-  if (rc) {
-    cudaEventDestroy(k0);
-    cudaEventDestroy(k1);
-    return rc;
+  if (!roots.empty())
+    DM_CUDA(cudaMemcpyAsync(ws.d_tasks, roots.data(), sizeof(int32_t) * roots.size(), cudaMemcpyHostToDevice, ctx.stream));
+  if (need_arena) {
+    L.arena_dcap = max_d + 4;
+    const size_t per_warp = (size_t)k * L.arena_dcap * sizeof(int32_t);
+    const size_t budget = (size_t)8 << 30;
+    ctx.arena_warps = (int)std::min<size_t>((size_t)clique_max_warps(ctx.num_sms), std::max<size_t>(8, budget / per_warp));
+    if ((rc = ensure_ws_bytes(&ws.d_scratch, &ws.scratch_cap, per_warp * ctx.arena_warps))) return rc;
+    L.arena = reinterpret_cast<int32_t*>(ws.d_scratch);
   }
-  DM_CUDA(cudaEventRecord(k1, ctx.stream));
+  const bool want_log = o && o->subtree_counts;
+  if (want_log) {
+    if ((rc = ensure_ws_bytes(reinterpret_cast<void**>(&ws.d_per_root), &ws.per_root_cap,
+                              sizeof(unsigned long long) * std::max(g->n, 1))))
+      return rc;
+    DM_CUDA(cudaMemsetAsync(ws.d_per_root, 0, sizeof(unsigned long long) * std::max(g->n, 1), ctx.stream));
+    L.per_root = ws.d_per_root;
+  }
+  if ((rc = init_counters(ws, (int)roots.size(), ctx.stream))) return rc;
+  L.g = GraphView{s->dg.d_orow, s->dg.d_odeg, s->dg.d_oadj, g->n};
+  L.roots = ws.d_tasks;
+  L.n_roots = (int)roots.size();
+  L.ctr = ws.d_ctr;
+  L.queue = ws.d_queue;
+  L.qcap = ws.qcap;
+  L.max_donations = ctx.donations_per_warp;
+  DM_CUDA(cudaEventRecord(ws.k0, ctx.stream));
+  int grid = 0;
+  if (!roots.empty()) {
+    rc = clique_launch(L, ctx, &grid);
+    if (rc) return rc;
+  }
+  DM_CUDA(cudaEventRecord(ws.k1, ctx.stream));
   DevCounters h;
   DM_CUDA(cudaMemcpyAsync(&h, ws.d_ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost, ctx.stream));
+  std::vector<unsigned long long> per_rank;
+  if (want_log) {
+    per_rank.resize(g->n);
+    if (g->n)
+      DM_CUDA(cudaMemcpyAsync(per_rank.data(), ws.d_per_root, sizeof(unsigned long long) * g->n, cudaMemcpyDeviceToHost,
+                              ctx.stream));
+  }
   DM_CUDA(cudaStreamSynchronize(ctx.stream));
+  if ((rc = reset_queue(ws, h, ctx.stream))) return rc;
   float kms = 0, pms = 0;
-  cudaEventElapsedTime(&kms, k0, k1);
-  cudaEventElapsedTime(&pms, ws.ev0, k0);
-  cudaEventDestroy(k0);
-  cudaEventDestroy(k1);
-  if (h.err) return fail(h.err == ERR_TIMEOUT ? DM_ETIMEOUT : DM_EOVERFLOW,
-                         "clique kernel reported error " + std::to_string(h.err));
+  cudaEventElapsedTime(&kms, ws.k0, ws.k1);
+  cudaEventElapsedTime(&pms, ws.ev0, ws.k0);
+  if (h.err)
+    return fail(h.err == ERR_TIMEOUT ? DM_ETIMEOUT : DM_EOVERFLOW,
+                "clique kernel reported error " + std::to_string(h.err));
   *count = h.count;
+  if (want_log)
+    for (int32_t v = 0; v < g->n; ++v) o->subtree_counts[v] = per_rank[g->rank[v]];
   if (st) {
     std::memset(st, 0, sizeof(*st));
     st->kernel_ms = kms;
@@ -336,7 +394,9 @@ int dm_count_cliques(dm_graph* g, int32_t k, const dm_opts* o, uint64_t* count, 
     st->donations = h.donations;
     st->idle_polls = h.idle_polls;
     st->nodes = h.nodes;
-    st->mode_used = tl.size() == roots.size() && !roots.empty() ? DM_MODE_LIST : DM_MODE_BITMAP;
+    st->mode_used = mode == DM_MODE_LIST ? DM_MODE_LIST : DM_MODE_BITMAP;
+    st->vwarp_used = 32;
+    st->grid = grid;
     st->block = 256;
     st->kernel_launches = ctx.launches;
   }

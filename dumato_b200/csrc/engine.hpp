@@ -10,17 +10,25 @@
 
 namespace dmb {
 
-// Per-call device counters. One instance lives in device memory for each call.
-struct DevCounters {
+// Per-call device counters and load-balancer state. One instance lives in device memory
+// for each call; the host initialises it (pending = number of root tasks). Words that
+// busy and hungry warps hit concurrently sit on separate 128-byte lines.
+struct alignas(128) DevCounters {
+  int cursor;                    // root cursor
+  int pad0[31];
+  int pending;                   // roots + donated tasks not finished yet
+  int pad1[31];
+  int hungry;                    // warps waiting for work
+  int pad2[31];
+  unsigned long long progress;   // work finished (batched), watched by waiting warps
+  unsigned long long pad3[15];
   unsigned long long count;      // clique total
   unsigned long long nodes;      // DFS nodes expanded
-  unsigned long long tasks;      // tasks executed
-  unsigned long long donations;  // donated work items
-  unsigned long long idle_polls;
-  int cursor[8];                 // task cursors (one per kernel)
+  unsigned long long tasks;      // tasks executed (roots + donated ranges)
+  unsigned long long donations;  // donated ranges
+  unsigned long long idle_polls; // polls of the donation queue by hungry warps
   int err;                       // first error code raised by a kernel (0 = none)
   int err_info;
-  int pad[6];
 };
 
 constexpr int ERR_ARENA_OVERFLOW = 1;
@@ -39,27 +47,34 @@ struct LaunchCtx {
   cudaStream_t stream = nullptr;
   int num_sms = 148;
   int launches = 0;
-  int timeout_ms = 2000;
+  int timeout_ms = 30000;
   int threads = 0;       // requested total threads (reference argv[3]); 0 = persistent default
   int block = 0;         // requested block size (reference argv[4]); 0 = kernel default
   int vwarp = 0;
-  int threshold = 100;   // donation trigger (idle percentage); >= 100 = off
+  int threshold = 0;     // donation trigger (hungry-warp percentage); >= 100 = off
   int donations_per_warp = 16;
+  int arena_warps = 0;   // warps the list arena has room for
+  int donate_after_us = 20;  // a task donates only after running this long
 };
 
-// Clique engine (clique.cu). tasks_* are device arrays of root ranks.
-struct CliqueTasks {
-  int32_t* d_thread1 = nullptr; int n_thread1 = 0;   // out-degree <= 64
-  int32_t* d_thread2 = nullptr; int n_thread2 = 0;   // 64 < out-degree <= 128
-  int32_t* d_warp = nullptr; int n_warp = 0;         // 128 < out-degree <= 2048
-  int32_t* d_list = nullptr; int n_list = 0;         // list-mode roots
-  int max_warp_deg = 0;
-  int max_list_deg = 0;
+// Clique engine (clique.cu).
+struct CliqueLaunch {
+  GraphView g;                   // degree-ordered DAG in rank space
+  int k = 0;
+  const int32_t* roots = nullptr;  // ordered root ranks
+  int n_roots = 0;
+  DevCounters* ctr = nullptr;
+  void* queue = nullptr;         // donation queue: header + slots (lb.cuh)
+  int qcap = 0;
+  int max_donations = 16;        // per task
+  int32_t* arena = nullptr;      // list path
+  int arena_dcap = 0;
+  int list_threshold = 256;
+  int nwmax = 1;
+  unsigned long long* per_root = nullptr;
 };
-
-int clique_launch(const GraphView& dag, int k, const CliqueTasks& t, DevCounters* d_ctr, LaunchCtx& ctx,
-                  void* d_scratch, size_t scratch_bytes, dm_stats* st);
-size_t clique_scratch_bytes(const CliqueTasks& t, int k, const LaunchCtx& ctx);
+int clique_launch(const CliqueLaunch& L, LaunchCtx& ctx, int* grid);
+int clique_max_warps(int num_sms);
 
 // Motif engine (motif.cu).
 struct MotifPlan {

@@ -1,0 +1,242 @@
+// Device-side warp-level load balancing: a root cursor, a lock-free donation queue and
+// termination detection, all inside one persistent kernel.
+//
+// This replaces the reference's host-mediated "stop the world" balancing
+// (src/main/DuMatoCPU.cu:386-562: poll d_status every 100 ms, raise d_stop, copy every
+// warp's stack to the host, donate (prefix, last extension) jobs from the heaviest warps
+// to idle ones, copy back, relaunch). Here a task is (root, item range): the items of a
+// root are the units its DFS is split into (local edges for cliques, second vertices for
+// motifs). A warp that finds the root cursor exhausted announces itself hungry; a busy
+// warp whose task has run for a while and sees hungry warps splits its remaining item
+// range in half and enqueues the upper half (a donated DFS prefix). The receiver rebuilds
+// the root's state and runs only the donated items.
+//
+// The queue is a bounded multi-producer multi-consumer ring (per-slot sequence numbers):
+// a consumer only ever takes a slot whose producer has finished writing it, so nothing
+// waits on another warp's store. Termination: `pending` counts roots not yet finished plus
+// donated tasks not yet finished (raised before the enqueue). A hungry warp leaves when
+// pending is zero; if nothing changes for timeout_ns it records ERR_TIMEOUT and leaves.
+//
+// Every hot word lives on its own 128-byte line so that polling hungry warps and busy
+// warps do not queue behind each other at one L2 slice.
+#pragma once
+
+#include <cstdint>
+
+#include "engine.hpp"
+
+namespace dmb {
+
+struct QSlot {
+  unsigned seq;
+  int root;
+  int begin;
+  int end;
+};
+
+// Persistent queue header, followed by `cap` slots. Positions keep running across calls
+// (a call ends with the queue empty); the host re-initialises it after an error.
+struct QHeader {
+  unsigned write_pos;
+  unsigned pad0[31];
+  unsigned read_pos;
+  unsigned pad1[31];
+};
+
+struct LBArgs {
+  DevCounters* ctr;
+  QHeader* qh;
+  QSlot* q;
+  int qcap;
+  int hungry_trigger;    // donate when at least this many warps are hungry (<= 0: never)
+  int max_donations;     // per task
+  long long donate_after_ns;  // a task donates only after running this long
+  long long timeout_ns;
+};
+
+__device__ __forceinline__ long long global_ns() {
+  long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ int vload(const int* p) { return *reinterpret_cast<const volatile int*>(p); }
+__device__ __forceinline__ unsigned vloadu(const unsigned* p) { return *reinterpret_cast<const volatile unsigned*>(p); }
+__device__ __forceinline__ unsigned long long vload64(const unsigned long long* p) {
+  return *reinterpret_cast<const volatile unsigned long long*>(p);
+}
+
+__device__ __forceinline__ void set_err(DevCounters* c, int code) { atomicCAS(&c->err, 0, code); }
+
+static __device__ __noinline__ bool q_push(const LBArgs& lb, int root, int b, int e) {
+  unsigned pos = vloadu(&lb.qh->write_pos);
+  QSlot* s;
+  for (int tries = 0; tries < 1024; ++tries) {
+    s = lb.q + (pos % (unsigned)lb.qcap);
+    const unsigned seq = vloadu(&s->seq);
+    const int dif = (int)(seq - pos);
+    if (dif == 0) {
+      const unsigned prev = atomicCAS(&lb.qh->write_pos, pos, pos + 1);
+      if (prev == pos) {
+        s->root = root;
+        s->begin = b;
+        s->end = e;
+        __threadfence();
+        atomicExch(&s->seq, pos + 1);
+        return true;
+      }
+      pos = prev;
+    } else if (dif < 0) {
+      return false;  // full
+    } else {
+      pos = vloadu(&lb.qh->write_pos);
+    }
+  }
+  return false;
+}
+
+static __device__ __noinline__ bool q_pop(const LBArgs& lb, int& root, int& b, int& e) {
+  unsigned pos = vloadu(&lb.qh->read_pos);
+  for (int tries = 0; tries < 1024; ++tries) {
+    QSlot* s = lb.q + (pos % (unsigned)lb.qcap);
+    const unsigned seq = vloadu(&s->seq);
+    const int dif = (int)(seq - (pos + 1));
+    if (dif == 0) {
+      const unsigned prev = atomicCAS(&lb.qh->read_pos, pos, pos + 1);
+      if (prev == pos) {
+        __threadfence();
+        const volatile QSlot* vs = s;
+        root = vs->root;
+        b = vs->begin;
+        e = vs->end;
+        __threadfence();
+        atomicExch(&s->seq, pos + (unsigned)lb.qcap);
+        return true;
+      }
+      pos = prev;
+    } else if (dif < 0) {
+      return false;  // empty (or a producer is still writing its slot)
+    } else {
+      pos = vloadu(&lb.qh->read_pos);
+    }
+  }
+  return false;
+}
+
+// Lane-0 only. Claims a chunk of roots [first, first+count) from the cursor, or failing
+// that a donated task (count = 1, range [b, e)). Returns false when all work is done or an
+// error was raised.
+static __device__ __noinline__ bool lb_next(const LBArgs& lb, int n_roots, int total_warps, int& first, int& count, int& b, int& e,
+                        bool& donated) {
+  DevCounters* c = lb.ctr;
+  int cur = vload(&c->cursor);
+  if (cur < n_roots) {
+    // light tail roots are claimed several at a time to keep the cursor line cool
+    int chunk = (n_roots - cur) / (8 * total_warps);
+    chunk = chunk < 1 ? 1 : (chunk > 16 ? 16 : chunk);
+    const int r = atomicAdd(&c->cursor, chunk);
+    if (r < n_roots) {
+      first = r;
+      count = min(chunk, n_roots - r);
+      b = 0;
+      e = -1;
+      donated = false;
+      return true;
+    }
+  }
+  atomicAdd(&c->hungry, 1);
+  long long t0 = global_ns();
+  unsigned long long last = vload64(&c->progress);
+  int last_pending = vload(&c->pending);
+  unsigned backoff = 256;
+  unsigned long long polls = 0;
+  bool got = false;
+  while (true) {
+    int root = 0;
+    if (q_pop(lb, root, b, e)) {
+      first = root;
+      count = 1;
+      donated = true;
+      got = true;
+      break;
+    }
+    const int pend = vload(&c->pending);
+    if (pend <= 0 || vload(&c->err) != 0) break;
+    const unsigned long long p = vload64(&c->progress);
+    if (p != last || pend != last_pending) {
+      last = p;
+      last_pending = pend;
+      t0 = global_ns();
+    } else if (global_ns() - t0 > lb.timeout_ns) {
+      set_err(c, ERR_TIMEOUT);
+      break;
+    }
+    ++polls;
+    __nanosleep(backoff);
+    if (backoff < 16384) backoff <<= 1;
+  }
+  atomicSub(&c->hungry, 1);
+  if (polls) atomicAdd(&c->idle_polls, polls);
+  return got;
+}
+
+__device__ __forceinline__ void lb_done(const LBArgs& lb, int count) {
+  __threadfence();
+  atomicSub(&lb.ctr->pending, count);
+}
+
+// Item range of the running task, packed as (next | end << 32) in shared memory. Taking an
+// item is one 64-bit atomicAdd (the low word is the cursor; it only ever passes `end` by
+// the number of lanes that find the range empty); splitting off a donation is one CAS.
+__device__ __forceinline__ unsigned long long pack_range(int next, int end) {
+  return (unsigned long long)(unsigned)next | ((unsigned long long)(unsigned)end << 32);
+}
+
+__device__ __forceinline__ int range_take(unsigned long long* range) {
+  const unsigned long long old = atomicAdd(range, 1ull);
+  const int next = (int)(unsigned)old, end = (int)(unsigned)(old >> 32);
+  return next < end ? next : -1;
+}
+
+// If warps are hungry and the task has run longer than donate_after_ns, splits the upper
+// half of the remaining range off and enqueues it. Returns true when the queue was full:
+// the split-off items [ob, oe) then belong to the caller, who must run them itself
+// (lanes that find the range empty have already moved the cursor past `mid`, so the split
+// cannot simply be undone). `busy` serialises donations of one warp.
+__device__ __forceinline__ bool range_maybe_donate(const LBArgs& lb, unsigned long long* range, int root,
+                                                   int* donations_left, long long task_start, int* busy, int& ob,
+                                                   int& oe) {
+  if (lb.hungry_trigger <= 0) return false;
+  if (*reinterpret_cast<volatile int*>(donations_left) <= 0) return false;
+  if (vload(&lb.ctr->hungry) < lb.hungry_trigger) return false;
+  if (global_ns() - task_start < lb.donate_after_ns) return false;
+  if (atomicCAS(busy, 0, 1) != 0) return false;
+  bool own = false;
+  unsigned long long cur = *reinterpret_cast<volatile unsigned long long*>(range);
+  while (true) {
+    const int next = (int)(unsigned)cur, end = (int)(unsigned)(cur >> 32);
+    if (end - next < 2) break;
+    const int mid = next + (end - next + 1) / 2;
+    const unsigned long long prev = atomicCAS(range, cur, pack_range(next, mid));
+    if (prev != cur) {
+      cur = prev;
+      continue;
+    }
+    atomicAdd(&lb.ctr->pending, 1);
+    if (q_push(lb, root, mid, end)) {
+      atomicSub(donations_left, 1);
+      atomicAdd(&lb.ctr->donations, 1ull);
+    } else {
+      atomicSub(&lb.ctr->pending, 1);
+      atomicExch(donations_left, 0);
+      ob = mid;
+      oe = end;
+      own = true;
+    }
+    break;
+  }
+  atomicExch(busy, 0);
+  return own;
+}
+
+}  // namespace dmb

@@ -101,8 +101,10 @@ typedef struct dm_opts {
   int32_t scheduler;           /* DM_SCHED_* */
   int32_t rank;                /* root shard: this process counts roots r with r % world == rank */
   int32_t world_size;          /* 0 or 1 = unsharded */
-  int32_t timeout_ms;          /* bound on every device-side wait (0 = 2000 ms) */
+  int32_t timeout_ms;          /* bound on every device-side wait without progress (0 = 30000 ms) */
   const void* predictor;       /* dm_predictor* for DM_SCHED_LEARNED, else NULL */
+  uint64_t* subtree_counts;    /* optional, n_vertices entries (original ids), overwritten: the
+                                  subgraphs counted under each root task (the subtree-size log) */
 } dm_opts;
 
 typedef struct dm_stats {

@@ -40,6 +40,7 @@ def lib() -> ctypes.CDLL:
             "oracle_clique_dfs_range": (ctypes.c_uint64, [_P, ctypes.c_int, ctypes.c_int32, ctypes.c_int32, ctypes.c_int]),
             "oracle_clique_brute": (ctypes.c_uint64, [_P, ctypes.c_int]),
             "oracle_clique_dag_bytes": (ctypes.c_uint64, [_P, ctypes.c_int, _P, ctypes.c_int]),
+            "oracle_clique_dag_per_root": (None, [_P, ctypes.c_int, _P, ctypes.c_int]),
             "oracle_motifs": (ctypes.c_int, [_P, ctypes.c_int, _P, ctypes.c_int32, _P, ctypes.c_int]),
             "oracle_motifs_range": (ctypes.c_int, [_P, ctypes.c_int, _P, ctypes.c_int32, _P, ctypes.c_int32,
                                                    ctypes.c_int32, ctypes.c_int, _P]),
@@ -104,6 +105,13 @@ def clique_dag_bytes(g: OracleGraph, k: int, threads: int = 0) -> tuple[int, int
     b = ctypes.c_uint64()
     c = lib().oracle_clique_dag_bytes(g.h, k, ctypes.byref(b), threads)
     return c, b.value
+
+
+def clique_per_root(g: OracleGraph, k: int, threads: int = 0) -> np.ndarray:
+    """k-cliques per root vertex (the clique's lowest (degree, id)-ranked vertex)."""
+    out = np.zeros(g.n, np.uint64)
+    lib().oracle_clique_dag_per_root(g.h, k, out.ctypes.data, threads)
+    return out
 
 
 def motifs(g: OracleGraph, k: int, q2c: np.ndarray, n_classes: int, threads: int = 0,

@@ -430,6 +430,7 @@ typedef struct {
   int32_t n;
   int64_t *off;
   int32_t *adj;
+  int32_t *orig; /* rank -> original id */
 } og_dag;
 
 static og_dag *make_dag(const og_graph *g) {
@@ -448,6 +449,8 @@ static og_dag *make_dag(const og_graph *g) {
   for (int32_t r = 0; r < n; ++r) rank[(uint32_t)key[r]] = r;
   og_dag *d = (og_dag *)calloc(1, sizeof(og_dag));
   d->n = n;
+  d->orig = (int32_t *)malloc(sizeof(int32_t) * (n + 1));
+  for (int32_t r = 0; r < n; ++r) d->orig[r] = (int32_t)(uint32_t)key[r];
   d->off = (int64_t *)calloc((size_t)n + 1, sizeof(int64_t));
   for (int32_t v = 0; v < n; ++v)
     for (int64_t e = g->off[v]; e < g->off[v + 1]; ++e) {
@@ -483,6 +486,7 @@ static og_dag *make_dag(const og_graph *g) {
 }
 
 static void free_dag(og_dag *d) {
+  free(d->orig);
   free(d->off);
   free(d->adj);
   free(d);
@@ -564,4 +568,29 @@ uint64_t oracle_clique_dag_bytes(const og_graph *g, int K, uint64_t *bytes_out, 
   free_dag(d);
   if (bytes_out) *bytes_out = bytes;
   return total;
+}
+
+/* Per-root K-clique counts on the degree-ordered DAG, indexed by original vertex id (the
+   root of a clique is its lowest-ranked vertex): the subtree size logged per task, used to
+   check the engine's logger and the work predictor. */
+void oracle_clique_dag_per_root(const og_graph *g, int K, uint64_t *per_root, int threads) {
+  og_dag *d = make_dag(g);
+  int32_t maxo = 0;
+  for (int32_t r = 0; r < d->n; ++r) {
+    int32_t x = (int32_t)(d->off[r + 1] - d->off[r]);
+    if (x > maxo) maxo = x;
+  }
+  int32_t cap = maxo + 1;
+#pragma omp parallel num_threads(resolve_threads(threads))
+  {
+    int32_t *buf = (int32_t *)malloc(sizeof(int32_t) * (size_t)cap * (K > 2 ? K : 2));
+#pragma omp for schedule(dynamic, 16)
+    for (int32_t r = 0; r < d->n; ++r) {
+      uint64_t c = 0, b = 0;
+      dag_clique_root(d, r, K, buf, cap, &c, &b);
+      per_root[d->orig[r]] = c;
+    }
+    free(buf);
+  }
+  free_dag(d);
 }

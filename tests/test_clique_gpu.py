@@ -102,3 +102,29 @@ def test_dense_roots_use_warp_and_list_modes(dm, orc, gpu):
         want = orc.clique_dag_bytes(og, k)[0]
         assert dm.count_cliques(g, k)[0] == want
         assert dm.count_cliques(g, k, dm.Options(mode=dm.MODE_LIST))[0] == want
+
+
+@pytest.mark.parametrize("k", [3, 5])
+def test_subtree_logger_matches_oracle(dm, orc, gpu, k):
+    from dumato_b200 import workloads
+
+    g = workloads.make("chunglu18k", 1)
+    og = _oracle_graph(orc, g)
+    per = np.zeros(g.info().n_vertices, np.uint64)
+    total, _ = dm.count_cliques(g, k, dm.Options(subtree_counts=per))
+    want = orc.clique_per_root(og, k)
+    assert int(per.sum()) == total
+    assert np.array_equal(per, want)
+
+
+def test_donations_happen_and_stay_exact(dm, orc, gpu):
+    from dumato_b200 import workloads
+
+    g = workloads.make("rmat100k", 1)
+    og = _oracle_graph(orc, g)
+    want, _ = orc.clique_dag_bytes(og, 5)
+    got, st = dm.count_cliques(g, 5, dm.Options(threshold=0))
+    assert got == want
+    assert st.donations > 0
+    off, _ = dm.count_cliques(g, 5, dm.Options(threshold=100))
+    assert off == want
