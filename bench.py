@@ -1,0 +1,333 @@
+"""Benchmark of the clique counting path: embeddings/s and time-to-count at k = 4..7.
+
+Workload (one "step"): k-clique counts for k = 4, 5, 6, 7 on the seeded Chung-Lu power-law
+graph of the benchmark configuration (18,700 vertices, 198,000 undirected edges, degree
+exponent 2.1, max degree 500), each count an exact uint64. `value` is embeddings/s: the
+cliques counted per second of device time-to-count, with the graph already resident in
+HBM. `e2e` is the same metric through the public C ABI with the graph re-uploaded from
+host memory every step (device copies released first) and the counts read back.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+With N > 1 (torchrun, one process per GPU) every rank counts its shard of the root tasks
+(roots in degree order, dealt round-robin) and the per-rank counts are summed with one
+all_reduce; the time is the max over ranks. `--impl reference` times the CPU port of the
+reference's plain DFS (OpenMP over roots) on the host cores instead.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+KS = (4, 5, 6, 7)
+WORKLOAD = "chunglu18k"
+SEED = 1
+FALLBACK_HBM_GBS = 6650.0
+REF_STRIDE = 64
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=300)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--scheduler", choices=["plain", "learned"], default="plain")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def measured_peak():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+        self.out = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(prefix="clocks", suffix=".csv")
+        os.close(fd)
+        try:
+            self.out = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=self.out, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        if self.out is not None:
+            self.out.close()
+
+    def summary(self):
+        if not self.path or not os.path.exists(self.path):
+            return None
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, flag in zip(names, parts[5:9]):
+                if flag.lower() in ("active", "1", "yes"):
+                    reasons.add(nm)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline(u, v):
+    """The oracle's OpenMP port of the reference's plain DFS, timed on this host's cores over
+    the full workload (every root, k = 4..7)."""
+    import oracle as orc
+
+    og = orc.OracleGraph.from_pairs(u, v)
+    threads = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    total = sum(orc.clique_dfs(og, k, threads=threads) for k in KS)
+    dt = time.perf_counter() - t0
+    return {"value": total / dt, "unit": "embeddings/s", "cores": threads, "kind": "port",
+            "sample": f"full workload: all {og.n} roots, k = 4..7, OpenMP dynamic schedule over roots"}
+
+
+def run_reference(args):
+    """CPU port of the reference's plain DFS on the host cores. One step = every 64th root id
+    (the offset rotates per step), k = 4..7; rank 0 only."""
+    world, rank, _ = dist_env()
+    if rank != 0:
+        return 0
+    import numpy as np
+
+    from dumato_b200 import workloads
+    import oracle as orc
+
+    g = workloads.make(WORKLOAD, SEED)
+    u, v = g.edges()
+    og = orc.OracleGraph.from_pairs(u, v)
+    threads = os.cpu_count() or 1
+    n = og.n
+    times, counts = [], []
+    for i in range(args.warmup + args.steps):
+        roots = np.arange(i % REF_STRIDE, n, REF_STRIDE, dtype=np.int32)
+        t0 = time.perf_counter()
+        c = sum(orc.clique_dfs_roots(og, k, roots, threads) for k in KS)
+        dt = time.perf_counter() - t0
+        if i >= args.warmup:
+            times.append(dt)
+            counts.append(c)
+    value = sum(counts) / sum(times)
+    sample = f"every {REF_STRIDE}th root id per step (offset rotates), k = 4..7, OpenMP dynamic schedule"
+    line = {
+        "impl": "reference", "metric": "embeddings/s", "value": value, "unit": "embeddings/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True, "scaling": "strong",
+        "vs_baseline": None, "dtype": "int64", "data": "synthetic (seeded Chung-Lu power-law graph)",
+        "config": {"workload": f"{WORKLOAD} k-cliques k=4..7", "vertices": int(n), "edges": int(og.m),
+                   "seed": SEED},
+        "cpu_baseline": {"value": value, "unit": "embeddings/s", "cores": threads, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": "embeddings/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    import torch
+
+    world, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+
+        import torch.distributed as tdist
+
+        tdist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    import dumato_b200 as dm
+    from dumato_b200 import workloads
+
+    g = workloads.make(WORKLOAD, SEED)
+    info = g.info()
+    stream = torch.cuda.current_stream()
+    sched = dm.SCHED_PLAIN if args.scheduler == "plain" else dm.SCHED_LEARNED
+    opts = dm.Options(device=local, stream=stream.cuda_stream, rank=rank, world_size=world, scheduler=sched)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.int32, device="cuda")
+
+    def step(collect=None):
+        total = 0
+        launches = 0
+        for k in KS:
+            c, st = dm.count_cliques(g, k, opts)
+            total += c
+            launches += st.kernel_launches
+            if collect is not None:
+                collect.append((k, c, st))
+        return total, launches
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+            torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        step()
+    # timed: device events around each step on the launching stream; L2 flushed before
+    # each step, outside the events
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    per_k = {k: [] for k in KS}
+    emb = 0
+    launches = 0
+    barrier()
+    with ClockSampler(local) as clocks:
+        for i in range(args.steps):
+            flush.zero_()
+            ev[i][0].record(stream)
+            coll = []
+            c, nl = step(coll)
+            ev[i][1].record(stream)
+            emb += c
+            launches += nl
+            for k, _, st in coll:
+                per_k[k].append(st.kernel_ms)
+        barrier()
+    t_total = sum(a.elapsed_time(b) for a, b in ev) / 1e3
+    if world > 1:
+        t = torch.tensor([t_total], dtype=torch.float64, device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        t_total = float(t.item())
+        e = torch.tensor([emb], dtype=torch.int64, device="cuda")
+        torch.distributed.all_reduce(e)
+        emb = int(e.item())
+    value = emb / t_total
+
+    # e2e: graph uploaded from host memory each step, counts read back, through the C ABI
+    e2e_steps = max(3, min(args.steps, 50))
+    e2e_emb = 0
+    e2e_ms = 0.0
+    barrier()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    for _ in range(e2e_steps):
+        g.release_device()
+        flush.zero_()
+        t0.record(stream)
+        c, _ = step()
+        t1.record(stream)
+        t1.synchronize()
+        e2e_ms += t0.elapsed_time(t1)
+        e2e_emb += c
+    n, m = info.n_vertices, info.n_edges
+    # padded oriented CSR (row starts, degrees, adjacency padded to 4-int rows), the root
+    # order, and the per-call counter block; the counter block is read back per call
+    h2d = 4 * 2 * n + 4 * (m + 3 * n) + 4 * n + 1024 * len(KS)
+    d2h = 1024 * len(KS)
+    e2e_t = e2e_ms / 1e3
+    if world > 1:
+        t = torch.tensor([e2e_t], dtype=torch.float64, device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_t = float(t.item())
+        e = torch.tensor([e2e_emb], dtype=torch.int64, device="cuda")
+        torch.distributed.all_reduce(e)
+        e2e_emb = int(e.item())
+    e2e_value = e2e_emb / e2e_t
+
+    # roofline of the counting kernel: algorithmic bytes per launch / mean launch duration
+    peak, peak_kind = measured_peak()
+    alg_bytes = {k: dm.clique_work_model(g, k)[1] for k in KS}
+    bytes_per_step = sum(alg_bytes.values()) / max(world, 1)
+    kern_s_per_step = sum(statistics.mean(per_k[k]) for k in KS) / 1e3
+    achieved = bytes_per_step / kern_s_per_step / 1e9
+    traffic = None
+    prof = ROOT / "profiles" / "clique_chunglu18k_traffic.json"
+    if prof.exists():
+        try:
+            traffic = json.loads(prof.read_text()).get("dram_bytes_per_step")
+        except Exception:
+            traffic = None
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        u, v = g.edges()
+        cpu = cpu_baseline(u, v)
+
+    if rank == 0:
+        line = {
+            "metric": "embeddings/s", "value": value, "unit": "embeddings/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t_total / args.steps,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "int64",
+            "data": "synthetic (seeded Chung-Lu power-law graph)",
+            "config": {"workload": f"{WORKLOAD} k-cliques k=4..7", "vertices": n, "edges": m,
+                       "max_degree": info.max_degree, "max_out_degree": info.max_out_degree, "seed": SEED,
+                       "scheduler": args.scheduler, "parallelism": f"root shards x{world}",
+                       "l2": "flushed before every step (256 MB write)"},
+            "time_to_count_ms": {str(k): statistics.mean(per_k[k]) for k in KS},
+            "embeddings_per_step": emb // max(args.steps, 1),
+            "gpu_launches": launches,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
+                         "algorithmic_bytes_per_step": bytes_per_step},
+            "e2e": {"value": e2e_value, "unit": "embeddings/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "steps": e2e_steps},
+            "cpu_baseline": cpu,
+            "clocks": clocks.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

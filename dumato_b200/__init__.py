@@ -92,6 +92,7 @@ _SIGNATURES = {
     "dm_dictionary_tables": (ctypes.c_int, [_P, _P, _P]),
     "dm_dictionary_connected": (ctypes.c_int, [_P, _P]),
     "dm_dictionary_free": (None, [_P]),
+    "dm_clique_work_model": (ctypes.c_int, [_P, ctypes.c_int32, _P, _P]),
     "dm_count_cliques": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.POINTER(_Opts), _P, ctypes.POINTER(_Stats)]),
     "dm_count_motifs": (ctypes.c_int, [_P, ctypes.c_int32, _P, ctypes.POINTER(_Opts), _P, ctypes.POINTER(_Stats)]),
 }
@@ -327,6 +328,15 @@ class Stats:
     def from_c(cls, s: _Stats) -> "Stats":
         return cls(s.kernel_ms, s.prep_ms, s.tasks, s.donations, s.idle_polls, s.nodes, s.mode_used,
                    s.vwarp_used, s.grid, s.block, s.kernel_launches)
+
+
+def clique_work_model(g: Graph, k: int) -> tuple[int, int]:
+    """(DFS nodes, algorithmic bytes) of k-clique counting on g's degree-ordered DAG; the
+    byte model behind the roofline figures (host-side accounting, not a counting path)."""
+    n = ctypes.c_uint64()
+    b = ctypes.c_uint64()
+    _check(lib().dm_clique_work_model(g.handle, int(k), ctypes.byref(n), ctypes.byref(b)))
+    return n.value, b.value
 
 
 def count_cliques(g: Graph, k: int, opts: Optional[Options] = None) -> tuple[int, Stats]:

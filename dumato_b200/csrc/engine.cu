@@ -68,6 +68,11 @@ static int init_queue(Workspace& ws, cudaStream_t st) {
 struct DeviceSlot {
   DeviceGraph dg;
   Workspace ws;
+  // roots (rank space) in descending out-degree order, resident on the device; the roots
+  // eligible for k-cliques (out-degree >= k-1) are a prefix of it
+  int32_t* d_deg_order = nullptr;
+  std::vector<int32_t> deg_order;
+  std::vector<int64_t> cnt_ge;  // cnt_ge[d] = roots with out-degree >= d
 };
 
 static std::mutex g_dev_mu;
@@ -211,6 +216,7 @@ void release_device_graphs(dm_graph* g) {
       cudaFree(s->ws.d_q2c);
       cudaFree(s->ws.d_queue);
       cudaFree(s->ws.d_per_root);
+      cudaFree(s->d_deg_order);
       if (s->ws.ev0) cudaEventDestroy(s->ws.ev0);
       if (s->ws.ev1) cudaEventDestroy(s->ws.ev1);
       if (s->ws.k0) cudaEventDestroy(s->ws.k0);
@@ -236,6 +242,26 @@ static int check_opts(const dm_opts* o) {
   if (o->block_size && (o->block_size % 32 || o->block_size > 1024))
     return fail(DM_EINVAL, "block_size must be a multiple of 32 up to 1024");
   if (o->scheduler == DM_SCHED_LEARNED && !o->predictor) return fail(DM_EINVAL, "learned scheduler needs a predictor");
+  return DM_OK;
+}
+
+// Descending out-degree order of all roots, uploaded once per (graph, device).
+static int ensure_deg_order(dm_graph* g, DeviceSlot* s, cudaStream_t st) {
+  if (s->d_deg_order) return DM_OK;
+  const int32_t n = g->n;
+  const int maxd = g->max_out_degree;
+  std::vector<int64_t> cnt((size_t)maxd + 2, 0);
+  for (int32_t r = 0; r < n; ++r) cnt[g->orow[r + 1] - g->orow[r]]++;
+  s->cnt_ge.assign((size_t)maxd + 2, 0);
+  for (int d = maxd; d >= 0; --d) s->cnt_ge[d] = s->cnt_ge[d + 1] + cnt[d];
+  // counting sort by descending degree, stable in rank
+  std::vector<int64_t> pos((size_t)maxd + 2, 0);
+  for (int d = 0; d <= maxd; ++d) pos[d] = s->cnt_ge[d + 1];
+  s->deg_order.assign(n, 0);
+  for (int32_t r = 0; r < n; ++r) s->deg_order[pos[g->orow[r + 1] - g->orow[r]]++] = r;
+  DM_CUDA(cudaMalloc(&s->d_deg_order, sizeof(int32_t) * std::max(n, 1)));
+  if (n)
+    DM_CUDA(cudaMemcpyAsync(s->d_deg_order, s->deg_order.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, st));
   return DM_OK;
 }
 
@@ -313,14 +339,26 @@ int dm_count_cliques(dm_graph* g, int32_t k, const dm_opts* o, uint64_t* count, 
   }
   // tasks: roots (rank space) with at least k-1 out-neighbours
   const int need = k - 1;
+  const int sched = o ? o->scheduler : DM_SCHED_PLAIN;
+  const int world = (o && o->world_size > 1) ? o->world_size : 1;
+  if ((rc = ensure_deg_order(g, s, ctx.stream))) return rc;
   std::vector<int32_t> roots;
-  roots.reserve(g->n);
-  for (int32_t r = 0; r < g->n; ++r)
-    if (g->orow[r + 1] - g->orow[r] >= need) roots.push_back(r);
-  if ((rc = order_roots(g, o, k, true, roots))) return rc;
+  const int32_t* d_roots = nullptr;
+  int n_roots = 0, max_d = 0;
+  if (sched == DM_SCHED_PLAIN && world == 1) {
+    // the eligible roots are a prefix of the cached descending-degree order
+    n_roots = need <= g->max_out_degree ? (int)s->cnt_ge[need] : 0;
+    d_roots = s->d_deg_order;
+    max_d = n_roots ? (int)(g->orow[s->deg_order[0] + 1] - g->orow[s->deg_order[0]]) : 0;
+  } else {
+    roots.reserve(g->n);
+    for (int32_t r = 0; r < g->n; ++r)
+      if (g->orow[r + 1] - g->orow[r] >= need) roots.push_back(r);
+    if ((rc = order_roots(g, o, k, true, roots))) return rc;
+    for (int32_t r : roots) max_d = std::max(max_d, (int)(g->orow[r + 1] - g->orow[r]));
+    n_roots = (int)roots.size();
+  }
   const int mode = o ? o->mode : DM_MODE_AUTO;
-  int max_d = 0;
-  for (int32_t r : roots) max_d = std::max(max_d, (int)(g->orow[r + 1] - g->orow[r]));
   CliqueLaunch L;
   L.k = k;
   if (mode == DM_MODE_LIST) {
@@ -331,10 +369,15 @@ int dm_count_cliques(dm_graph* g, int32_t k, const dm_opts* o, uint64_t* count, 
     L.list_threshold = 64 * L.nwmax;
   }
   const bool need_arena = max_d > L.list_threshold && k > 3;
-  if ((rc = ensure_ws_bytes(reinterpret_cast<void**>(&ws.d_tasks), &ws.tasks_cap, sizeof(int32_t) * (roots.size() + 1))))
-    return rc;
-  if (!roots.empty())
-    DM_CUDA(cudaMemcpyAsync(ws.d_tasks, roots.data(), sizeof(int32_t) * roots.size(), cudaMemcpyHostToDevice, ctx.stream));
+  if (!d_roots) {
+    if ((rc = ensure_ws_bytes(reinterpret_cast<void**>(&ws.d_tasks), &ws.tasks_cap,
+                              sizeof(int32_t) * (roots.size() + 1))))
+      return rc;
+    if (!roots.empty())
+      DM_CUDA(cudaMemcpyAsync(ws.d_tasks, roots.data(), sizeof(int32_t) * roots.size(), cudaMemcpyHostToDevice,
+                              ctx.stream));
+    d_roots = ws.d_tasks;
+  }
   if (need_arena) {
     L.arena_dcap = max_d + 4;
     const size_t per_warp = (size_t)k * L.arena_dcap * sizeof(int32_t);
@@ -351,17 +394,17 @@ int dm_count_cliques(dm_graph* g, int32_t k, const dm_opts* o, uint64_t* count, 
     DM_CUDA(cudaMemsetAsync(ws.d_per_root, 0, sizeof(unsigned long long) * std::max(g->n, 1), ctx.stream));
     L.per_root = ws.d_per_root;
   }
-  if ((rc = init_counters(ws, (int)roots.size(), ctx.stream))) return rc;
+  if ((rc = init_counters(ws, n_roots, ctx.stream))) return rc;
   L.g = GraphView{s->dg.d_orow, s->dg.d_odeg, s->dg.d_oadj, g->n};
-  L.roots = ws.d_tasks;
-  L.n_roots = (int)roots.size();
+  L.roots = d_roots;
+  L.n_roots = n_roots;
   L.ctr = ws.d_ctr;
   L.queue = ws.d_queue;
   L.qcap = ws.qcap;
   L.max_donations = ctx.donations_per_warp;
   DM_CUDA(cudaEventRecord(ws.k0, ctx.stream));
   int grid = 0;
-  if (!roots.empty()) {
+  if (n_roots > 0) {
     rc = clique_launch(L, ctx, &grid);
     if (rc) return rc;
   }

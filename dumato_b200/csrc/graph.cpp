@@ -452,6 +452,59 @@ int dm_graph_write_edgelist(const dm_graph* g, const char* path) {
   return DM_OK;
 }
 
+int dm_clique_work_model(dm_graph* g, int32_t k, uint64_t* nodes_out, uint64_t* bytes_out) {
+  if (!g || !nodes_out || !bytes_out) return fail(DM_EINVAL, "dm_clique_work_model: null argument");
+  if (k < 2 || k > 12) return fail(DM_EINVAL, "dm_clique_work_model: k must be in [2, 12]");
+  {
+    std::lock_guard<std::mutex> lk(g->mu);
+    ensure_oriented(g);
+  }
+  const int32_t n = g->n;
+  uint64_t nodes = 0, bytes = 0;
+  const size_t cap = (size_t)g->max_out_degree + 1;
+  std::vector<int32_t> buf(cap * k);
+  std::vector<int32_t*> C(k);
+  std::vector<int32_t> nC(k), pos(k);
+  for (int i = 0; i < k; ++i) C[i] = buf.data() + (size_t)i * cap;
+  for (int32_t r = 0; r < n; ++r) {
+    const int32_t na = (int32_t)(g->orow[r + 1] - g->orow[r]);
+    std::copy(g->oadj.begin() + g->orow[r], g->oadj.begin() + g->orow[r + 1], C[0]);
+    nC[0] = na;
+    ++nodes;
+    bytes += 8ull * (uint64_t)na;
+    if (k == 2) continue;
+    int l = 0;
+    pos[0] = 0;
+    while (l >= 0) {
+      if (l == k - 2 || pos[l] >= nC[l]) {
+        --l;
+        continue;
+      }
+      const int32_t v = C[l][pos[l]++];
+      const int32_t* B = g->oadj.data() + g->orow[v];
+      const int32_t nb = (int32_t)(g->orow[v + 1] - g->orow[v]);
+      int32_t i = pos[l], j = 0, m = 0;
+      while (i < nC[l] && j < nb) {
+        if (C[l][i] < B[j]) ++i;
+        else if (C[l][i] > B[j]) ++j;
+        else {
+          C[l + 1][m++] = C[l][i];
+          ++i;
+          ++j;
+        }
+      }
+      ++nodes;
+      bytes += 4ull * ((uint64_t)nC[l] + (uint64_t)nb) + 4ull * (uint64_t)m;
+      ++l;
+      nC[l] = m;
+      pos[l] = 0;
+    }
+  }
+  *nodes_out = nodes;
+  *bytes_out = bytes;
+  return DM_OK;
+}
+
 void dm_graph_free(dm_graph* g) {
   if (!g) return;
   release_device_graphs(g);

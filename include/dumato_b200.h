@@ -160,6 +160,12 @@ DM_API int dm_count_cliques(dm_graph* g, int32_t k, const dm_opts* opts, uint64_
 DM_API int dm_count_motifs(dm_graph* g, int32_t k, const dm_dictionary* dict, const dm_opts* opts,
                     uint64_t* class_counts, dm_stats* stats);
 
+/* Work model of the clique path (host-side, for roofline accounting only; it is not a
+   counting path): on the degree-ordered DAG, every DFS node at levels 0..k-2 that computes
+   a candidate set C_child = C_parent cap N+(v) costs 4(|C_parent| + |N+(v)|) + 4|C_child|
+   bytes (level 0: 4|N+(v0)| + 4|C_0|). Writes the node count and the byte total. */
+DM_API int dm_clique_work_model(dm_graph* g, int32_t k, uint64_t* nodes, uint64_t* bytes);
+
 /* Release this library's device copies of g on its device (host CSR stays). */
 DM_API int dm_graph_release_device(dm_graph* g);
 

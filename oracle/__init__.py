@@ -38,6 +38,7 @@ def lib() -> ctypes.CDLL:
             "oracle_graph_maxdeg": (ctypes.c_int32, [_P]),
             "oracle_clique_dfs": (ctypes.c_uint64, [_P, ctypes.c_int, ctypes.c_int]),
             "oracle_clique_dfs_range": (ctypes.c_uint64, [_P, ctypes.c_int, ctypes.c_int32, ctypes.c_int32, ctypes.c_int]),
+            "oracle_clique_dfs_roots": (ctypes.c_uint64, [_P, ctypes.c_int, _P, ctypes.c_int64, ctypes.c_int]),
             "oracle_clique_brute": (ctypes.c_uint64, [_P, ctypes.c_int]),
             "oracle_clique_dag_bytes": (ctypes.c_uint64, [_P, ctypes.c_int, _P, ctypes.c_int]),
             "oracle_clique_dag_per_root": (None, [_P, ctypes.c_int, _P, ctypes.c_int]),
@@ -95,6 +96,11 @@ def clique_dfs(g: OracleGraph, k: int, threads: int = 0, root_begin: int = 0, ro
     if root_end < 0:
         root_end = g.n
     return lib().oracle_clique_dfs_range(g.h, k, root_begin, root_end, threads)
+
+
+def clique_dfs_roots(g: OracleGraph, k: int, roots, threads: int = 0) -> int:
+    r = np.ascontiguousarray(roots, dtype=np.int32)
+    return lib().oracle_clique_dfs_roots(g.h, k, r.ctypes.data, r.size, threads)
 
 
 def clique_brute(g: OracleGraph, k: int) -> int:

@@ -594,3 +594,13 @@ void oracle_clique_dag_per_root(const og_graph *g, int K, uint64_t *per_root, in
   }
   free_dag(d);
 }
+
+/* Plain DFS over an explicit list of roots (the bounded samples of the CPU baseline). */
+uint64_t oracle_clique_dfs_roots(const og_graph *g, int K, const int32_t *roots, int64_t n_roots, int threads) {
+  if (K < 1 || K > 31) return 0;
+  uint64_t total = 0;
+#pragma omp parallel for schedule(dynamic, 1) reduction(+ : total) num_threads(resolve_threads(threads))
+  for (int64_t i = 0; i < n_roots; ++i)
+    if (roots[i] >= 0 && roots[i] < g->n) total += clique_root(g, roots[i], K);
+  return total;
+}
