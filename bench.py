@@ -33,7 +33,7 @@ KS = (4, 5, 6, 7)
 WORKLOAD = "chunglu18k"
 SEED = 1
 FALLBACK_HBM_GBS = 6650.0
-REF_STRIDE = 64
+REF_STRIDE = 256
 
 
 def parse_args():
@@ -138,7 +138,7 @@ def cpu_baseline(u, v):
 
 
 def run_reference(args):
-    """CPU port of the reference's plain DFS on the host cores. One step = every 64th root id
+    """CPU port of the reference's plain DFS on the host cores. One step = every 256th root id
     (the offset rotates per step), k = 4..7; rank 0 only."""
     world, rank, _ = dist_env()
     if rank != 0:

@@ -15,6 +15,7 @@
 // max-code equals nauty's canonical code, so the tables are identical to the reference's;
 // for k >= 5 the partition of quick codes is identical and only the id order may differ.
 #include <algorithm>
+#include <atomic>
 #include <cstdio>
 #include <cstring>
 #include <map>
@@ -26,6 +27,8 @@
 namespace dmb {
 
 static inline int quick_bits(int k) { return k * (k - 1) / 2 - 1; }
+
+static std::atomic<uint64_t> g_dict_uid{1};
 
 // adjacency as k row bitmasks
 struct Small {
@@ -135,6 +138,7 @@ int dm_dictionary_generate(int32_t k, dm_dictionary** out) {
   for (int32_t r = 0; r < nc; ++r) rank_of[order[r]] = r;
   dm_dictionary* d = new (std::nothrow) dm_dictionary();
   if (!d) return fail(DM_ENOMEM, "out of host memory");
+  d->uid = g_dict_uid++;
   d->k = k;
   d->n_quicks = nq;
   d->n_classes = nc;
@@ -175,6 +179,7 @@ int dm_dictionary_load_csv(const char* path, dm_dictionary** out) {
     if ((1ll << quick_bits(kk)) == nq) k = kk;
   if (!k) return bad("quick count is not 2^(k(k-1)/2-1) for k in [3,7]");
   dm_dictionary* d = new dm_dictionary();
+  d->uid = g_dict_uid++;
   d->k = k;
   d->n_quicks = nq;
   d->quick_to_class.assign(nq, -1);

@@ -66,6 +66,7 @@ struct dm_graph {
 };
 
 struct dm_dictionary {
+  uint64_t uid = 0;                      // unique per dictionary object (device table cache key)
   int32_t k = 0;
   int64_t n_quicks = 0;
   int32_t n_classes = 0;

@@ -35,7 +35,7 @@ struct Workspace {
   size_t hist_cap = 0;
   int32_t* d_q2c = nullptr;
   size_t q2c_cap = 0;
-  const void* q2c_owner = nullptr;  // dictionary whose table is resident
+  uint64_t q2c_uid = 0;             // dictionary whose table is resident
   void* d_queue = nullptr;          // donation queue, ready flags kept zero between calls
   int qcap = 0;
   unsigned long long* d_per_root = nullptr;
@@ -73,6 +73,9 @@ struct DeviceSlot {
   int32_t* d_deg_order = nullptr;
   std::vector<int32_t> deg_order;
   std::vector<int64_t> cnt_ge;  // cnt_ge[d] = roots with out-degree >= d
+  // motif roots (vertices with a neighbour above them) by descending upper degree
+  int32_t* d_up_order = nullptr;
+  int n_up = 0;
 };
 
 static std::mutex g_dev_mu;
@@ -217,6 +220,7 @@ void release_device_graphs(dm_graph* g) {
       cudaFree(s->ws.d_queue);
       cudaFree(s->ws.d_per_root);
       cudaFree(s->d_deg_order);
+      cudaFree(s->d_up_order);
       if (s->ws.ev0) cudaEventDestroy(s->ws.ev0);
       if (s->ws.ev1) cudaEventDestroy(s->ws.ev1);
       if (s->ws.k0) cudaEventDestroy(s->ws.k0);
@@ -438,6 +442,146 @@ int dm_count_cliques(dm_graph* g, int32_t k, const dm_opts* o, uint64_t* count, 
     st->idle_polls = h.idle_polls;
     st->nodes = h.nodes;
     st->mode_used = mode == DM_MODE_LIST ? DM_MODE_LIST : DM_MODE_BITMAP;
+    st->vwarp_used = 32;
+    st->grid = grid;
+    st->block = 256;
+    st->kernel_launches = ctx.launches;
+  }
+  return DM_OK;
+}
+
+int dm_count_motifs(dm_graph* g, int32_t k, const dm_dictionary* dict, const dm_opts* o, uint64_t* class_counts,
+                    dm_stats* st) {
+  if (!g || !dict || !class_counts) return fail(DM_EINVAL, "dm_count_motifs: null argument");
+  if (k < 3 || k > 7) return fail(DM_EINVAL, "dm_count_motifs: k must be in [3, 7]");
+  if (dict->k != k) return fail(DM_EINVAL, "dm_count_motifs: dictionary was built for another k");
+  int rc = check_opts(o);
+  if (rc) return rc;
+  LaunchCtx ctx;
+  rc = select_device(o, ctx);
+  if (rc) return rc;
+  std::lock_guard<std::mutex> lk(g->mu);
+  DeviceSlot* s = slot_for(g, ctx.device);
+  Workspace& ws = s->ws;
+  if ((rc = prepare_ws(ws, ctx.stream))) return rc;
+  DM_CUDA(cudaEventRecord(ws.ev0, ctx.stream));
+  if (!s->dg.has_undirected) {
+    rc = upload_csr(g->row, g->adj, g->n, &s->dg.d_row, &s->dg.d_deg, &s->dg.d_adj, ctx.stream);
+    if (rc) return rc;
+    s->dg.has_undirected = true;
+  }
+  auto upper = [&](int32_t v) {
+    const int32_t* b = g->adj.data() + g->row[v];
+    const int32_t* e = g->adj.data() + g->row[v + 1];
+    return (int)(e - std::upper_bound(b, e, v));
+  };
+  const int sched = o ? o->scheduler : DM_SCHED_PLAIN;
+  const int world = (o && o->world_size > 1) ? o->world_size : 1;
+  const int32_t* d_roots = nullptr;
+  int n_roots = 0;
+  if (!s->d_up_order) {
+    std::vector<int32_t> order;
+    for (int32_t v = 0; v < g->n; ++v)
+      if (upper(v) > 0) order.push_back(v);
+    std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) { return upper(a) > upper(b); });
+    DM_CUDA(cudaMalloc(&s->d_up_order, sizeof(int32_t) * std::max<size_t>(order.size(), 1)));
+    if (!order.empty())
+      DM_CUDA(cudaMemcpyAsync(s->d_up_order, order.data(), sizeof(int32_t) * order.size(), cudaMemcpyHostToDevice,
+                              ctx.stream));
+    DM_CUDA(cudaStreamSynchronize(ctx.stream));
+    s->n_up = (int)order.size();
+  }
+  std::vector<int32_t> roots;
+  if (sched == DM_SCHED_PLAIN && world == 1) {
+    d_roots = s->d_up_order;
+    n_roots = s->n_up;
+  } else {
+    for (int32_t v = 0; v < g->n; ++v)
+      if (upper(v) > 0) roots.push_back(v);
+    if (sched == DM_SCHED_PLAIN)
+      std::stable_sort(roots.begin(), roots.end(), [&](int32_t a, int32_t b) { return upper(a) > upper(b); });
+    if ((rc = order_roots(g, o, k, false, roots))) return rc;
+    n_roots = (int)roots.size();
+    if ((rc = ensure_ws_bytes(reinterpret_cast<void**>(&ws.d_tasks), &ws.tasks_cap,
+                              sizeof(int32_t) * (roots.size() + 1))))
+      return rc;
+    if (!roots.empty())
+      DM_CUDA(cudaMemcpyAsync(ws.d_tasks, roots.data(), sizeof(int32_t) * roots.size(), cudaMemcpyHostToDevice,
+                              ctx.stream));
+    d_roots = ws.d_tasks;
+  }
+  // dictionary table
+  if (ws.q2c_uid != dict->uid) {
+    if ((rc = ensure_ws_bytes(reinterpret_cast<void**>(&ws.d_q2c), &ws.q2c_cap, sizeof(int32_t) * dict->n_quicks)))
+      return rc;
+    DM_CUDA(cudaMemcpyAsync(ws.d_q2c, dict->quick_to_class.data(), sizeof(int32_t) * dict->n_quicks,
+                            cudaMemcpyHostToDevice, ctx.stream));
+    ws.q2c_uid = dict->uid;
+  }
+  if ((rc = ensure_ws_bytes(reinterpret_cast<void**>(&ws.d_hist), &ws.hist_cap,
+                            sizeof(unsigned long long) * dict->n_classes)))
+    return rc;
+  DM_CUDA(cudaMemsetAsync(ws.d_hist, 0, sizeof(unsigned long long) * dict->n_classes, ctx.stream));
+  // arena: extension levels and runs per warp
+  const int maxdeg = std::max(g->max_degree, 1);
+  const size_t per_warp = motif_arena_stride(k, maxdeg) * sizeof(int2);
+  const size_t budget = (size_t)8 << 30;
+  ctx.arena_warps = (int)std::min<size_t>((size_t)ctx.num_sms * 64, std::max<size_t>(8, budget / per_warp));
+  if ((rc = ensure_ws_bytes(&ws.d_scratch, &ws.scratch_cap, per_warp * ctx.arena_warps))) return rc;
+  const bool want_log = o && o->subtree_counts;
+  if (want_log) {
+    if ((rc = ensure_ws_bytes(reinterpret_cast<void**>(&ws.d_per_root), &ws.per_root_cap,
+                              sizeof(unsigned long long) * std::max(g->n, 1))))
+      return rc;
+    DM_CUDA(cudaMemsetAsync(ws.d_per_root, 0, sizeof(unsigned long long) * std::max(g->n, 1), ctx.stream));
+  }
+  if ((rc = init_counters(ws, n_roots, ctx.stream))) return rc;
+  MotifLaunch L;
+  L.g = GraphView{s->dg.d_row, s->dg.d_deg, s->dg.d_adj, g->n};
+  L.k = k;
+  L.roots = d_roots;
+  L.n_roots = n_roots;
+  L.ctr = ws.d_ctr;
+  L.queue = ws.d_queue;
+  L.qcap = ws.qcap;
+  L.max_donations = ctx.donations_per_warp;
+  L.q2c = ws.d_q2c;
+  L.n_classes = dict->n_classes;
+  L.hist = ws.d_hist;
+  L.arena = ws.d_scratch;
+  L.maxdeg = maxdeg;
+  L.per_root = want_log ? ws.d_per_root : nullptr;
+  DM_CUDA(cudaEventRecord(ws.k0, ctx.stream));
+  int grid = 0;
+  if (n_roots > 0) {
+    rc = motif_launch(L, ctx, &grid);
+    if (rc) return rc;
+  }
+  DM_CUDA(cudaEventRecord(ws.k1, ctx.stream));
+  DevCounters h;
+  DM_CUDA(cudaMemcpyAsync(&h, ws.d_ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost, ctx.stream));
+  DM_CUDA(cudaMemcpyAsync(class_counts, ws.d_hist, sizeof(unsigned long long) * dict->n_classes,
+                          cudaMemcpyDeviceToHost, ctx.stream));
+  if (want_log && g->n)
+    DM_CUDA(cudaMemcpyAsync(o->subtree_counts, ws.d_per_root, sizeof(unsigned long long) * g->n,
+                            cudaMemcpyDeviceToHost, ctx.stream));
+  DM_CUDA(cudaStreamSynchronize(ctx.stream));
+  if ((rc = reset_queue(ws, h, ctx.stream))) return rc;
+  float kms = 0, pms = 0;
+  cudaEventElapsedTime(&kms, ws.k0, ws.k1);
+  cudaEventElapsedTime(&pms, ws.ev0, ws.k0);
+  if (h.err)
+    return fail(h.err == ERR_TIMEOUT ? DM_ETIMEOUT : DM_EOVERFLOW,
+                "motif kernel reported error " + std::to_string(h.err));
+  if (st) {
+    std::memset(st, 0, sizeof(*st));
+    st->kernel_ms = kms;
+    st->prep_ms = pms;
+    st->tasks = h.tasks;
+    st->donations = h.donations;
+    st->idle_polls = h.idle_polls;
+    st->nodes = h.nodes;
+    st->mode_used = DM_MODE_LIST;
     st->vwarp_used = 32;
     st->grid = grid;
     st->block = 256;

@@ -77,19 +77,24 @@ int clique_launch(const CliqueLaunch& L, LaunchCtx& ctx, int* grid);
 int clique_max_warps(int num_sms);
 
 // Motif engine (motif.cu).
-struct MotifPlan {
+struct MotifLaunch {
+  GraphView g;                   // undirected CSR, original ids
   int k = 0;
+  const int32_t* roots = nullptr;
+  int n_roots = 0;
+  DevCounters* ctr = nullptr;
+  void* queue = nullptr;
+  int qcap = 0;
+  int max_donations = 16;
+  const int32_t* q2c = nullptr;
   int n_classes = 0;
-  const int32_t* d_q2c = nullptr;        // quick -> class
-  unsigned long long* d_hist = nullptr;  // n_classes
-  int32_t* d_tasks = nullptr;            // roots
-  int n_tasks = 0;
-  int max_deg = 0;
+  unsigned long long* hist = nullptr;
+  void* arena = nullptr;
+  int maxdeg = 0;
+  unsigned long long* per_root = nullptr;
 };
-
-int motif_launch(const GraphView& g, const MotifPlan& p, DevCounters* d_ctr, LaunchCtx& ctx, void* d_scratch,
-                 size_t scratch_bytes, dm_stats* st);
-size_t motif_scratch_bytes(const MotifPlan& p, const LaunchCtx& ctx, int* warps_out);
+int motif_launch(const MotifLaunch& L, LaunchCtx& ctx, int* grid);
+size_t motif_arena_stride(int k, int maxdeg);  // int2 slots per warp
 
 const char* cuda_err_str(cudaError_t e);
 
