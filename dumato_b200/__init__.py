@@ -93,6 +93,8 @@ _SIGNATURES = {
     "dm_dictionary_connected": (ctypes.c_int, [_P, _P]),
     "dm_dictionary_free": (None, [_P]),
     "dm_clique_work_model": (ctypes.c_int, [_P, ctypes.c_int32, _P, _P]),
+    "dm_count_cliques_noalloc": (ctypes.c_int, [_P, _P, _P, ctypes.c_int32, _P, ctypes.c_int32, ctypes.c_int32,
+                                                ctypes.c_int32, ctypes.c_uint64, _P]),
     "dm_count_cliques": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.POINTER(_Opts), _P, ctypes.POINTER(_Stats)]),
     "dm_count_motifs": (ctypes.c_int, [_P, ctypes.c_int32, _P, ctypes.POINTER(_Opts), _P, ctypes.POINTER(_Stats)]),
 }

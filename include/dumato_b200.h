@@ -166,6 +166,25 @@ DM_API int dm_count_motifs(dm_graph* g, int32_t k, const dm_dictionary* dict, co
    bytes (level 0: 4|N+(v0)| + 4|C_0|). Writes the node count and the byte total. */
 DM_API int dm_clique_work_model(dm_graph* g, int32_t k, uint64_t* nodes, uint64_t* bytes);
 
+/* k-cliques of a DAG already in device memory, with no GPU allocation (no counterpart in
+   the reference). For callers that cannot call cudaMalloc: code that runs inside another
+   framework's memory pool or an allocator-free runtime, or that must not change the
+   device's allocation state. Inputs (device pointers, current device): d_row[v] start of
+   v's out-neighbours in d_adj, d_deg[v] their number; every row sorted ascending and
+   holding only ids greater than v (for example, an undirected graph keeping u -> v for
+   u < v); d_roots[0..n_roots) the vertices to start from (each clique is counted from its
+   lowest vertex, so pass every vertex whose out-degree is at least k-1). max_out_degree
+   must be at most 256: larger roots need per-warp scratch this entry point does not hold
+   (use dm_count_cliques). Output: *count (host). Runs on `stream` and waits for it.
+   Scratch: one fixed device array of about 260 KB (counters + donation queue) that every
+   GPU loading the library keeps until exit. The first call on a device resolves its
+   address and initialises it, so make that first call before any stream capture. Calls
+   share the array: calls that overlap on the GPU (other streams, threads or processes
+   sharing the context) race and must be serialised by the caller. */
+DM_API int dm_count_cliques_noalloc(const int32_t* d_row, const int32_t* d_deg, const int32_t* d_adj,
+                                    int32_t n_vertices, const int32_t* d_roots, int32_t n_roots,
+                                    int32_t max_out_degree, int32_t k, uint64_t stream, uint64_t* count);
+
 /* Release this library's device copies of g on its device (host CSR stays). */
 DM_API int dm_graph_release_device(dm_graph* g);
 
