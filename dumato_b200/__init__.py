@@ -93,6 +93,16 @@ _SIGNATURES = {
     "dm_dictionary_connected": (ctypes.c_int, [_P, _P]),
     "dm_dictionary_free": (None, [_P]),
     "dm_clique_work_model": (ctypes.c_int, [_P, ctypes.c_int32, _P, _P]),
+    "dm_predictor_create": (ctypes.c_int, [ctypes.c_uint64, ctypes.POINTER(_P)]),
+    "dm_predictor_free": (None, [_P]),
+    "dm_predictor_num_params": (ctypes.c_int, []),
+    "dm_predictor_get_params": (ctypes.c_int, [_P, _P]),
+    "dm_predictor_set_params": (ctypes.c_int, [_P, _P]),
+    "dm_predictor_features": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_int32, _P]),
+    "dm_predictor_predict": (ctypes.c_int, [_P, _P, ctypes.c_int64, _P]),
+    "dm_predictor_gradients": (ctypes.c_int, [_P, _P, _P, ctypes.c_int64, _P, _P]),
+    "dm_predictor_train": (ctypes.c_int, [_P, _P, _P, ctypes.c_int64, ctypes.c_int32, ctypes.c_int32,
+                                          ctypes.c_float, _P]),
     "dm_count_cliques_noalloc": (ctypes.c_int, [_P, _P, _P, ctypes.c_int32, _P, ctypes.c_int32, ctypes.c_int32,
                                                 ctypes.c_int32, ctypes.c_uint64, _P]),
     "dm_count_cliques": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.POINTER(_Opts), _P, ctypes.POINTER(_Stats)]),
@@ -278,6 +288,91 @@ class Dictionary:
                 self._h = None
         except Exception:
             pass
+
+
+class Predictor:
+    """Learned work predictor: an 8 -> 32 -> 32 -> 1 FP32 MLP over root-task features,
+    trained and evaluated by the library's CUDA kernels (log(1 + subtree size) target)."""
+
+    N_FEATURES = 8
+
+    def __init__(self, seed: int = 0):
+        h = _P()
+        _check(lib().dm_predictor_create(int(seed), ctypes.byref(h)))
+        self._h = h
+
+    @property
+    def handle(self) -> int:
+        return self._h.value
+
+    @property
+    def n_params(self) -> int:
+        return lib().dm_predictor_num_params()
+
+    def get_params(self) -> np.ndarray:
+        p = np.empty(self.n_params, np.float32)
+        _check(lib().dm_predictor_get_params(self._h, _ptr(p)))
+        return p
+
+    def set_params(self, params: np.ndarray) -> None:
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        if p.size != self.n_params:
+            raise ValueError(f"expected {self.n_params} parameters")
+        _check(lib().dm_predictor_set_params(self._h, _ptr(p)))
+
+    @staticmethod
+    def features(g: "Graph", k: int, clique: bool = True) -> np.ndarray:
+        X = np.empty((g.info().n_vertices, Predictor.N_FEATURES), np.float32)
+        _check(lib().dm_predictor_features(g.handle, int(k), 1 if clique else 0, _ptr(X)))
+        return X
+
+    def predict(self, X: np.ndarray) -> np.ndarray:
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        y = np.empty(X.shape[0], np.float32)
+        _check(lib().dm_predictor_predict(self._h, _ptr(X), X.shape[0], _ptr(y)))
+        return y
+
+    def gradients(self, X: np.ndarray, T: np.ndarray) -> tuple[np.ndarray, float]:
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        T = np.ascontiguousarray(T, dtype=np.float32)
+        g = np.empty(self.n_params, np.float32)
+        loss = ctypes.c_float()
+        _check(lib().dm_predictor_gradients(self._h, _ptr(X), _ptr(T), X.shape[0], _ptr(g), ctypes.byref(loss)))
+        return g, loss.value
+
+    def train(self, X: np.ndarray, T: np.ndarray, epochs: int = 60, batch: int = 256, lr: float = 3e-3) -> float:
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        T = np.ascontiguousarray(T, dtype=np.float32)
+        loss = ctypes.c_float()
+        _check(lib().dm_predictor_train(self._h, _ptr(X), _ptr(T), X.shape[0], int(epochs), int(batch),
+                                        float(lr), ctypes.byref(loss)))
+        return loss.value
+
+    def __del__(self):
+        try:
+            if self._h:
+                lib().dm_predictor_free(self._h)
+                self._h = None
+        except Exception:
+            pass
+
+
+def subtree_log(g: "Graph", k: int, clique: bool = True, dictionary: "Optional[Dictionary]" = None):
+    """Per-root subtree sizes logged by the plain engine: (features[n, 8], log1p(size)[n],
+    roots mask). Roots that start no task are masked out."""
+    n = g.info().n_vertices
+    per = np.zeros(n, np.uint64)
+    opts = Options(subtree_counts=per)
+    if clique:
+        count_cliques(g, k, opts)
+    else:
+        count_motifs(g, k, dictionary, opts)
+    X = Predictor.features(g, k, clique)
+    if clique:
+        mask = np.expm1(X[:, 5]).round() >= k - 1        # DAG out-degree >= k-1
+    else:
+        mask = np.expm1(X[:, 2]).round() >= 1            # a neighbour above v
+    return X, np.log1p(per.astype(np.float64)).astype(np.float32), mask
 
 
 @dataclass

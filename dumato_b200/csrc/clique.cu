@@ -118,6 +118,7 @@ struct CliqueArgs {
   const int32_t* roots;
   int n_roots;
   LBArgs lb;
+  const int32_t* parts;         // optional per-root-entry part word (p | P << 16), else null
   int32_t* arena;               // list path: K * arena_dcap ints per warp
   int arena_dcap;
   int list_threshold;           // roots with d > list_threshold take the list path
@@ -284,9 +285,10 @@ __device__ unsigned long long bitmap_task(const CliqueArgs& a, unsigned char* ws
   } else {
     n_items = d;
   }
-  const int hi = e < 0 ? n_items : min(e, n_items);
+  int lo, hi;
+  task_range(b, e, n_items, lo, hi);
   if (lane == 0) {
-    *range = pack_range(b, hi);
+    *range = pack_range(lo, hi);
     *donations_left = a.lb.max_donations;
     *busy = 0;
     *hn = 0;
@@ -332,9 +334,10 @@ __device__ unsigned long long list_task(const CliqueArgs& a, unsigned char* wsm,
   int* sN = reinterpret_cast<int*>(wsm + LY.n);
   int* sPos = reinterpret_cast<int*>(wsm + LY.pos);
   const int32_t* L = a.g.adj + __ldg(a.g.row + root);
-  const int hi = e < 0 ? d : min(e, d);
+  int lo, hi;
+  task_range(b, e, d, lo, hi);
   if (lane == 0) {
-    *range = pack_range(b, hi);
+    *range = pack_range(lo, hi);
     *donations_left = a.lb.max_donations;
     *busy = 0;
   }
@@ -449,6 +452,8 @@ __global__ void __launch_bounds__(256) clique_kernel(CliqueArgs a) {
     donated = __shfl_sync(FULL_MASK, donated ? 1 : 0, 0) != 0;
     for (int ti = 0; ti < count; ++ti) {
       const int root = donated ? first : __ldg(a.roots + first + ti);
+      int bb = b, ee = e;
+      if (!donated && a.parts) part_bounds(__ldg(a.parts + first + ti), bb, ee);
       ++ntasks;
       unsigned long long task_cnt = 0;
       const int d = __ldg(a.g.deg + root);
@@ -460,14 +465,14 @@ __global__ void __launch_bounds__(256) clique_kernel(CliqueArgs a) {
         if (K > 3 && (!my_arena || d > a.arena_dcap)) {
           if (lane == 0) set_err(a.lb.ctr, ERR_ARENA_OVERFLOW);
         } else {
-          task_cnt = list_task<K, M>(a, wsm, root, d, b, e, my_arena);
+          task_cnt = list_task<K, M>(a, wsm, root, d, bb, ee, my_arena);
         }
       } else {
         const int nw = (d + 63) >> 6;
-        if (nw <= 1) task_cnt = bitmap_task<K, 1, M>(a, wsm, root, d, b, e);
-        else if (M >= 2 && nw == 2) task_cnt = bitmap_task<K, (M >= 2 ? 2 : 1), M>(a, wsm, root, d, b, e);
-        else if (M >= 3 && nw == 3) task_cnt = bitmap_task<K, (M >= 3 ? 3 : 1), M>(a, wsm, root, d, b, e);
-        else if (M >= 4 && nw == 4) task_cnt = bitmap_task<K, (M >= 4 ? 4 : 1), M>(a, wsm, root, d, b, e);
+        if (nw <= 1) task_cnt = bitmap_task<K, 1, M>(a, wsm, root, d, bb, ee);
+        else if (M >= 2 && nw == 2) task_cnt = bitmap_task<K, (M >= 2 ? 2 : 1), M>(a, wsm, root, d, bb, ee);
+        else if (M >= 3 && nw == 3) task_cnt = bitmap_task<K, (M >= 3 ? 3 : 1), M>(a, wsm, root, d, bb, ee);
+        else if (M >= 4 && nw == 4) task_cnt = bitmap_task<K, (M >= 4 ? 4 : 1), M>(a, wsm, root, d, bb, ee);
         else if (lane == 0) set_err(a.lb.ctr, ERR_BAD_TASK);
       }
       cnt += task_cnt;
@@ -536,6 +541,7 @@ int clique_launch(const CliqueLaunch& L, LaunchCtx& ctx, int* grid) {
   a.arena_dcap = L.arena_dcap;
   a.list_threshold = L.list_threshold;
   a.per_root = L.per_root;
+  a.parts = L.parts;
   switch (L.k) {
     case 2: return launch_nw<2>(a, L.nwmax, ctx, grid);
     case 3: return launch_nw<3>(a, L.nwmax, ctx, grid);

@@ -60,6 +60,8 @@ struct dm_graph {
   std::vector<int64_t> orow;     // n+1 (rank space)
   std::vector<int32_t> oadj;     // m
   int32_t max_out_degree = 0;
+  // k-independent predictor features per vertex (6 per vertex), for cliques and motifs
+  std::vector<float> feat[2];
   // device copies
   std::mutex mu;
   std::vector<dmb::DeviceGraph*> dev;

@@ -40,6 +40,8 @@ struct Workspace {
   int qcap = 0;
   unsigned long long* d_per_root = nullptr;
   size_t per_root_cap = 0;
+  int32_t* d_parts = nullptr;       // scheduler part words, parallel to the task list
+  size_t parts_cap = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, k0 = nullptr, k1 = nullptr;
 };
 
@@ -219,6 +221,7 @@ void release_device_graphs(dm_graph* g) {
       cudaFree(s->ws.d_q2c);
       cudaFree(s->ws.d_queue);
       cudaFree(s->ws.d_per_root);
+      cudaFree(s->ws.d_parts);
       cudaFree(s->d_deg_order);
       cudaFree(s->d_up_order);
       if (s->ws.ev0) cudaEventDestroy(s->ws.ev0);
@@ -231,6 +234,16 @@ void release_device_graphs(dm_graph* g) {
     delete s;
   }
   g->dev.clear();
+}
+
+static int upload_parts(Workspace& ws, const std::vector<int32_t>& parts, cudaStream_t st, const int32_t** out) {
+  *out = nullptr;
+  if (parts.empty()) return DM_OK;
+  int rc = ensure_ws_bytes(reinterpret_cast<void**>(&ws.d_parts), &ws.parts_cap, sizeof(int32_t) * parts.size());
+  if (rc) return rc;
+  DM_CUDA(cudaMemcpyAsync(ws.d_parts, parts.data(), sizeof(int32_t) * parts.size(), cudaMemcpyHostToDevice, st));
+  *out = ws.d_parts;
+  return DM_OK;
 }
 
 static int check_opts(const dm_opts* o) {
@@ -272,30 +285,48 @@ static int ensure_deg_order(dm_graph* g, DeviceSlot* s, cudaStream_t st) {
 // Root order (shared by both engines): plain = descending degree (heaviest first), id =
 // ascending vertex id (the reference's round-robin striping order, DuMatoCPU.cu:126-135),
 // learned = descending predicted cost. The shard keeps every world_size-th task.
-int predictor_order(const void* predictor, dm_graph* g, int k, bool clique, std::vector<int32_t>& roots);
+int predictor_schedule(const void* pv, dm_graph* g, int k, bool clique, int total_warps, std::vector<int32_t>& roots,
+                       std::vector<int32_t>& parts);
+int ensure_features(dm_graph* g, bool clique);
 
-static int order_roots(dm_graph* g, const dm_opts* o, int k, bool clique, std::vector<int32_t>& roots) {
+static int order_roots(dm_graph* g, const dm_opts* o, int k, bool clique, int total_warps,
+                       std::vector<int32_t>& roots, std::vector<int32_t>& parts) {
   const int sched = o ? o->scheduler : DM_SCHED_PLAIN;
+  parts.clear();
   if (sched == DM_SCHED_LEARNED) {
-    int rc = predictor_order(o->predictor, g, k, clique, roots);
+    int rc = predictor_schedule(o->predictor, g, k, clique, total_warps, roots, parts);
     if (rc) return rc;
   } else if (sched == DM_SCHED_ID) {
-    if (clique) std::sort(roots.begin(), roots.end(), [&](int32_t a, int32_t b) { return a < b; });
+    if (clique) {
+      // rank space -> ascending original id
+      std::vector<int32_t> inv(g->n);
+      for (int32_t v = 0; v < g->n; ++v) inv[g->rank[v]] = v;
+      std::sort(roots.begin(), roots.end(), [&](int32_t a, int32_t b) { return inv[a] < inv[b]; });
+    } else {
+      std::sort(roots.begin(), roots.end());
+    }
   } else {
     if (clique) {
       std::stable_sort(roots.begin(), roots.end(), [&](int32_t a, int32_t b) {
         return g->orow[a + 1] - g->orow[a] > g->orow[b + 1] - g->orow[b];
       });
     } else {
-      std::stable_sort(roots.begin(), roots.end(), [&](int32_t a, int32_t b) {
-        return g->row[a + 1] - g->row[a] > g->row[b + 1] - g->row[b];
-      });
+      auto upper = [&](int32_t v) {
+        const int32_t* b = g->adj.data() + g->row[v];
+        const int32_t* e = g->adj.data() + g->row[v + 1];
+        return e - std::upper_bound(b, e, v);
+      };
+      std::stable_sort(roots.begin(), roots.end(), [&](int32_t a, int32_t b) { return upper(a) > upper(b); });
     }
   }
   if (o && o->world_size > 1) {
-    std::vector<int32_t> mine;
-    for (size_t i = o->rank; i < roots.size(); i += o->world_size) mine.push_back(roots[i]);
+    std::vector<int32_t> mine, mparts;
+    for (size_t i = o->rank; i < roots.size(); i += o->world_size) {
+      mine.push_back(roots[i]);
+      if (!parts.empty()) mparts.push_back(parts[i]);
+    }
     roots.swap(mine);
+    parts.swap(mparts);
   }
   return DM_OK;
 }
@@ -330,6 +361,7 @@ int dm_count_cliques(dm_graph* g, int32_t k, const dm_opts* o, uint64_t* count, 
   LaunchCtx ctx;
   rc = select_device(o, ctx);
   if (rc) return rc;
+  if (o && o->scheduler == DM_SCHED_LEARNED && (rc = ensure_features(g, true))) return rc;
   std::lock_guard<std::mutex> lk(g->mu);
   ensure_oriented(g);
   DeviceSlot* s = slot_for(g, ctx.device);
@@ -346,7 +378,7 @@ int dm_count_cliques(dm_graph* g, int32_t k, const dm_opts* o, uint64_t* count, 
   const int sched = o ? o->scheduler : DM_SCHED_PLAIN;
   const int world = (o && o->world_size > 1) ? o->world_size : 1;
   if ((rc = ensure_deg_order(g, s, ctx.stream))) return rc;
-  std::vector<int32_t> roots;
+  std::vector<int32_t> roots, parts;
   const int32_t* d_roots = nullptr;
   int n_roots = 0, max_d = 0;
   if (sched == DM_SCHED_PLAIN && world == 1) {
@@ -358,10 +390,12 @@ int dm_count_cliques(dm_graph* g, int32_t k, const dm_opts* o, uint64_t* count, 
     roots.reserve(g->n);
     for (int32_t r = 0; r < g->n; ++r)
       if (g->orow[r + 1] - g->orow[r] >= need) roots.push_back(r);
-    if ((rc = order_roots(g, o, k, true, roots))) return rc;
+    if ((rc = order_roots(g, o, k, true, ctx.num_sms * 32, roots, parts))) return rc;
     for (int32_t r : roots) max_d = std::max(max_d, (int)(g->orow[r + 1] - g->orow[r]));
     n_roots = (int)roots.size();
   }
+  const int32_t* d_parts = nullptr;
+  if ((rc = upload_parts(ws, parts, ctx.stream, &d_parts))) return rc;
   const int mode = o ? o->mode : DM_MODE_AUTO;
   CliqueLaunch L;
   L.k = k;
@@ -401,6 +435,7 @@ int dm_count_cliques(dm_graph* g, int32_t k, const dm_opts* o, uint64_t* count, 
   if ((rc = init_counters(ws, n_roots, ctx.stream))) return rc;
   L.g = GraphView{s->dg.d_orow, s->dg.d_odeg, s->dg.d_oadj, g->n};
   L.roots = d_roots;
+  L.parts = d_parts;
   L.n_roots = n_roots;
   L.ctr = ws.d_ctr;
   L.queue = ws.d_queue;
@@ -460,6 +495,7 @@ int dm_count_motifs(dm_graph* g, int32_t k, const dm_dictionary* dict, const dm_
   LaunchCtx ctx;
   rc = select_device(o, ctx);
   if (rc) return rc;
+  if (o && o->scheduler == DM_SCHED_LEARNED && (rc = ensure_features(g, false))) return rc;
   std::lock_guard<std::mutex> lk(g->mu);
   DeviceSlot* s = slot_for(g, ctx.device);
   Workspace& ws = s->ws;
@@ -491,16 +527,14 @@ int dm_count_motifs(dm_graph* g, int32_t k, const dm_dictionary* dict, const dm_
     DM_CUDA(cudaStreamSynchronize(ctx.stream));
     s->n_up = (int)order.size();
   }
-  std::vector<int32_t> roots;
+  std::vector<int32_t> roots, parts;
   if (sched == DM_SCHED_PLAIN && world == 1) {
     d_roots = s->d_up_order;
     n_roots = s->n_up;
   } else {
     for (int32_t v = 0; v < g->n; ++v)
       if (upper(v) > 0) roots.push_back(v);
-    if (sched == DM_SCHED_PLAIN)
-      std::stable_sort(roots.begin(), roots.end(), [&](int32_t a, int32_t b) { return upper(a) > upper(b); });
-    if ((rc = order_roots(g, o, k, false, roots))) return rc;
+    if ((rc = order_roots(g, o, k, false, ctx.num_sms * 32, roots, parts))) return rc;
     n_roots = (int)roots.size();
     if ((rc = ensure_ws_bytes(reinterpret_cast<void**>(&ws.d_tasks), &ws.tasks_cap,
                               sizeof(int32_t) * (roots.size() + 1))))
@@ -536,7 +570,10 @@ int dm_count_motifs(dm_graph* g, int32_t k, const dm_dictionary* dict, const dm_
     DM_CUDA(cudaMemsetAsync(ws.d_per_root, 0, sizeof(unsigned long long) * std::max(g->n, 1), ctx.stream));
   }
   if ((rc = init_counters(ws, n_roots, ctx.stream))) return rc;
+  const int32_t* d_parts = nullptr;
+  if ((rc = upload_parts(ws, parts, ctx.stream, &d_parts))) return rc;
   MotifLaunch L;
+  L.parts = d_parts;
   L.g = GraphView{s->dg.d_row, s->dg.d_deg, s->dg.d_adj, g->n};
   L.k = k;
   L.roots = d_roots;

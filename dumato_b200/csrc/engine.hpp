@@ -72,6 +72,7 @@ struct CliqueLaunch {
   int list_threshold = 256;
   int nwmax = 1;
   unsigned long long* per_root = nullptr;
+  const int32_t* parts = nullptr;   // per root entry: p | P << 16 (0 = whole root)
 };
 int clique_launch(const CliqueLaunch& L, LaunchCtx& ctx, int* grid);
 int clique_max_warps(int num_sms);
@@ -92,6 +93,7 @@ struct MotifLaunch {
   void* arena = nullptr;
   int maxdeg = 0;
   unsigned long long* per_root = nullptr;
+  const int32_t* parts = nullptr;
 };
 int motif_launch(const MotifLaunch& L, LaunchCtx& ctx, int* grid);
 size_t motif_arena_stride(int k, int maxdeg);  // int2 slots per warp

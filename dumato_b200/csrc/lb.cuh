@@ -185,6 +185,28 @@ __device__ __forceinline__ void lb_done(const LBArgs& lb, int count) {
   atomicSub(&lb.ctr->pending, count);
 }
 
+// Item range of a task over n items. Donated ranges are [b, e) (e < 0: to the end). A root
+// pre-split by the scheduler into P parts is encoded b = -1 - p, e = -1 - P and covers
+// [p*n/P, (p+1)*n/P); whole roots come as (0, -1).
+__device__ __forceinline__ void task_range(int b, int e, int n, int& lo, int& hi) {
+  if (b < 0) {
+    const int p = -1 - b, P = -1 - e;
+    lo = (int)((long long)p * n / P);
+    hi = (int)((long long)(p + 1) * n / P);
+  } else {
+    lo = b;
+    hi = e < 0 ? n : min(e, n);
+  }
+}
+
+// Decodes a scheduler part word (p | P << 16; 0 = the whole root) into (b, e).
+__device__ __forceinline__ void part_bounds(int part, int& b, int& e) {
+  if (part) {
+    b = -1 - (part & 0xffff);
+    e = -1 - (part >> 16);
+  }
+}
+
 // Item range of the running task, packed as (next | end << 32) in shared memory. Taking an
 // item is one 64-bit atomicAdd (the low word is the cursor; it only ever passes `end` by
 // the number of lanes that find the range empty); splitting off a donation is one CAS.

@@ -51,6 +51,7 @@ struct MotifArgs {
   int arena_stride;            // int2 slots per warp
   int maxdeg;
   unsigned long long* per_root;
+  const int32_t* parts;        // optional per-root-entry part word (p | P << 16)
 };
 
 __host__ __device__ constexpr int quick_off(int p) { return (p - 2) * (p + 1) / 2; }
@@ -147,6 +148,8 @@ __global__ void __launch_bounds__(32 * MOTIF_WARPS) motif_kernel(MotifArgs a) {
     donated = __shfl_sync(FULL_MASK, donated ? 1 : 0, 0) != 0;
     for (int ti = 0; ti < count; ++ti) {
       const int v0 = donated ? first : __ldg(a.roots + first + ti);
+      int bb = b, ee = e;
+      if (!donated && a.parts) part_bounds(__ldg(a.parts + first + ti), bb, ee);
       ++ntasks;
       unsigned long long task_cnt = 0;
       const long long t_start = global_ns();
@@ -156,9 +159,10 @@ __global__ void __launch_bounds__(32 * MOTIF_WARPS) motif_kernel(MotifArgs a) {
       const int s0 = lower_bound(row0, 0, deg0, v0 + 1);
       const int32_t* E0 = row0 + s0;
       const int n0 = deg0 - s0;
-      const int hi = e < 0 ? n0 : min(e, n0);
+      int lo, hi;
+      task_range(bb, ee, n0, lo, hi);
       if (lane == 0) {
-        sw->range = pack_range(b, hi);
+        sw->range = pack_range(lo, hi);
         sw->donations_left = a.lb.max_donations;
         sw->busy = 0;
         sw->quick[0] = 0;
@@ -376,6 +380,7 @@ int motif_launch(const MotifLaunch& L, LaunchCtx& ctx, int* grid) {
   a.arena_stride = (int)motif_arena_stride(L.k, L.maxdeg);
   a.maxdeg = L.maxdeg;
   a.per_root = L.per_root;
+  a.parts = L.parts;
   switch (L.k) {
     case 3: return launch_motif<3>(a, ctx, grid);
     case 4: return launch_motif<4>(a, ctx, grid);

@@ -53,6 +53,7 @@ extern "C" {
 
 typedef struct dm_graph dm_graph;
 typedef struct dm_dictionary dm_dictionary;
+typedef struct dm_predictor dm_predictor;
 
 /* Graph generators (seeded, deterministic on every platform). */
 #define DM_GEN_ER 0        /* G(n, m): m distinct undirected pairs, no self-loops */
@@ -184,6 +185,27 @@ DM_API int dm_clique_work_model(dm_graph* g, int32_t k, uint64_t* nodes, uint64_
 DM_API int dm_count_cliques_noalloc(const int32_t* d_row, const int32_t* d_deg, const int32_t* d_adj,
                                     int32_t n_vertices, const int32_t* d_roots, int32_t n_roots,
                                     int32_t max_out_degree, int32_t k, uint64_t stream, uint64_t* count);
+
+/* ---- learned work predictor (no counterpart in the reference) ----
+   An 8 -> 32 -> 32 -> 1 FP32 MLP predicting log(1 + subtree size) of a root task, trained
+   and evaluated by this library's CUDA kernels. Pass it as dm_opts.predictor with
+   scheduler = DM_SCHED_LEARNED to order root tasks by predicted cost and pre-split the
+   predicted-heavy ones. */
+DM_API int dm_predictor_create(uint64_t seed, dm_predictor** out);
+DM_API void dm_predictor_free(dm_predictor* p);
+DM_API int dm_predictor_num_params(void);
+DM_API int dm_predictor_get_params(const dm_predictor* p, float* params);
+DM_API int dm_predictor_set_params(dm_predictor* p, const float* params);
+/* features[n_vertices * 8] of every vertex as a root of a k query (clique != 0: clique
+   tasks, else motif tasks) */
+DM_API int dm_predictor_features(dm_graph* g, int32_t k, int32_t clique, float* features);
+DM_API int dm_predictor_predict(const dm_predictor* p, const float* X, int64_t n, float* y);
+/* gradient of the mean squared error over (X, T) (one full batch), and the loss */
+DM_API int dm_predictor_gradients(const dm_predictor* p, const float* X, const float* T, int64_t n, float* grad,
+                                  float* loss);
+/* Adam over shuffled minibatches for `epochs` passes; writes the last epoch's mean loss */
+DM_API int dm_predictor_train(dm_predictor* p, const float* X, const float* T, int64_t n, int32_t epochs,
+                              int32_t batch, float lr, float* final_loss);
 
 /* Release this library's device copies of g on its device (host CSR stays). */
 DM_API int dm_graph_release_device(dm_graph* g);
