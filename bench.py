@@ -179,6 +179,53 @@ def run_reference(args):
     return 0
 
 
+LVP_WORKLOAD = "rmat100k"
+LVP_KS = (6, 7)
+
+
+def learned_vs_plain(dm, workloads, reps: int = 5):
+    """Time-to-count of the learned scheduler against plain device balancing on the skewed
+    R-MAT workload (k = 6, 7). The predictor is trained on subtree sizes logged by the
+    plain engine on two other seeds of the same configuration; the learned time includes
+    its scheduling (feature rows, inference, ordering, splitting)."""
+    import numpy as np
+
+    t0 = time.perf_counter()
+    Xs, Ts = [], []
+    for s in (2, 3):
+        g2 = workloads.make(LVP_WORKLOAD, s)
+        for k in (4, 5, 6, 7):
+            X, T, m = dm.subtree_log(g2, k)
+            Xs.append(X[m])
+            Ts.append(T[m])
+    pr = dm.Predictor(seed=1)
+    loss = pr.train(np.concatenate(Xs), np.concatenate(Ts), epochs=40, batch=512, lr=3e-3)
+    train_s = time.perf_counter() - t0
+    g = workloads.make(LVP_WORKLOAD, SEED)
+    out = {"workload": f"{LVP_WORKLOAD} k-cliques", "train_seeds": [2, 3], "test_seed": SEED,
+           "train_loss": loss, "train_s": train_s, "by_k": {}}
+    for k in LVP_KS:
+        X, T, m = dm.subtree_log(g, k)
+        mae = float(np.mean(np.abs(pr.predict(X[m]) - T[m])))
+        res = {}
+        for name, opts in (("plain", dm.Options()),
+                           ("learned", dm.Options(scheduler=dm.SCHED_LEARNED, predictor=pr.handle))):
+            ms, idle, cnt = [], [], None
+            dm.count_cliques(g, k, opts)
+            for _ in range(reps):
+                c, st = dm.count_cliques(g, k, opts)
+                ms.append(st.kernel_ms + st.prep_ms)
+                idle.append(st.idle_warp_fraction)
+                cnt = c
+            res[name] = {"time_to_count_ms": statistics.median(ms), "idle_warp_fraction": statistics.median(idle),
+                         "count": cnt}
+        assert res["plain"]["count"] == res["learned"]["count"]
+        res["speedup"] = res["plain"]["time_to_count_ms"] / res["learned"]["time_to_count_ms"]
+        res["mae_log_subtree"] = mae
+        out["by_k"][str(k)] = res
+    return out
+
+
 def main():
     args = parse_args()
     if args.impl == "reference":
@@ -298,9 +345,11 @@ def main():
             traffic = None
 
     cpu = None
+    lvp = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         u, v = g.edges()
         cpu = cpu_baseline(u, v)
+        lvp = learned_vs_plain(dm, workloads)
 
     if rank == 0:
         line = {
@@ -322,6 +371,7 @@ def main():
             "e2e": {"value": e2e_value, "unit": "embeddings/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "steps": e2e_steps},
             "cpu_baseline": cpu,
+            "learned_vs_plain": lvp,
             "clocks": clocks.summary(),
         }
         print(json.dumps(line), flush=True)

@@ -68,7 +68,8 @@ class _Stats(ctypes.Structure):
     _fields_ = [("kernel_ms", ctypes.c_double), ("prep_ms", ctypes.c_double), ("tasks", ctypes.c_uint64),
                 ("donations", ctypes.c_uint64), ("idle_polls", ctypes.c_uint64), ("nodes", ctypes.c_uint64),
                 ("mode_used", ctypes.c_int32), ("vwarp_used", ctypes.c_int32), ("grid", ctypes.c_int32),
-                ("block", ctypes.c_int32), ("kernel_launches", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+                ("block", ctypes.c_int32), ("kernel_launches", ctypes.c_int32), ("reserved", ctypes.c_int32),
+                ("idle_warp_fraction", ctypes.c_double)]
 
 
 _P = ctypes.c_void_p
@@ -420,11 +421,12 @@ class Stats:
     grid: int = 0
     block: int = 0
     kernel_launches: int = 0
+    idle_warp_fraction: float = 0.0
 
     @classmethod
     def from_c(cls, s: _Stats) -> "Stats":
         return cls(s.kernel_ms, s.prep_ms, s.tasks, s.donations, s.idle_polls, s.nodes, s.mode_used,
-                   s.vwarp_used, s.grid, s.block, s.kernel_launches)
+                   s.vwarp_used, s.grid, s.block, s.kernel_launches, s.idle_warp_fraction)
 
 
 def clique_work_model(g: Graph, k: int) -> tuple[int, int]:

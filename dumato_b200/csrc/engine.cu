@@ -481,6 +481,8 @@ int dm_count_cliques(dm_graph* g, int32_t k, const dm_opts* o, uint64_t* count, 
     st->grid = grid;
     st->block = 256;
     st->kernel_launches = ctx.launches;
+    const double warp_ns = (double)grid * 8.0 * (double)kms * 1e6;
+    st->idle_warp_fraction = warp_ns > 0 ? std::min(1.0, (double)h.hungry_ns / warp_ns) : 0.0;
   }
   return DM_OK;
 }
@@ -623,6 +625,8 @@ int dm_count_motifs(dm_graph* g, int32_t k, const dm_dictionary* dict, const dm_
     st->grid = grid;
     st->block = 256;
     st->kernel_launches = ctx.launches;
+    const double warp_ns = (double)grid * 8.0 * (double)kms * 1e6;
+    st->idle_warp_fraction = warp_ns > 0 ? std::min(1.0, (double)h.hungry_ns / warp_ns) : 0.0;
   }
   return DM_OK;
 }

@@ -27,6 +27,7 @@ struct alignas(128) DevCounters {
   unsigned long long tasks;      // tasks executed (roots + donated ranges)
   unsigned long long donations;  // donated ranges
   unsigned long long idle_polls; // polls of the donation queue by hungry warps
+  unsigned long long hungry_ns;  // time warps spent waiting for work, summed over warps
   int err;                       // first error code raised by a kernel (0 = none)
   int err_info;
 };

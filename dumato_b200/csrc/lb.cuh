@@ -145,7 +145,8 @@ static __device__ __noinline__ bool lb_next(const LBArgs& lb, int n_roots, int t
     }
   }
   atomicAdd(&c->hungry, 1);
-  long long t0 = global_ns();
+  const long long t_hungry = global_ns();
+  long long t0 = t_hungry;
   unsigned long long last = vload64(&c->progress);
   int last_pending = vload(&c->pending);
   unsigned backoff = 256;
@@ -177,6 +178,7 @@ static __device__ __noinline__ bool lb_next(const LBArgs& lb, int n_roots, int t
   }
   atomicSub(&c->hungry, 1);
   if (polls) atomicAdd(&c->idle_polls, polls);
+  atomicAdd(&c->hungry_ns, (unsigned long long)(global_ns() - t_hungry));
   return got;
 }
 
@@ -221,13 +223,14 @@ __device__ __forceinline__ int range_take(unsigned long long* range) {
 }
 
 // If warps are hungry and the task has run longer than donate_after_ns, splits the upper
-// half of the remaining range off and enqueues it. Returns true when the queue was full:
+// half of the remaining range off and enqueues it (with cost_tail > 0, item i is taken to
+// cost cost_tail - i and the split halves the remaining cost instead of the item count). Returns true when the queue was full:
 // the split-off items [ob, oe) then belong to the caller, who must run them itself
 // (lanes that find the range empty have already moved the cursor past `mid`, so the split
 // cannot simply be undone). `busy` serialises donations of one warp.
 __device__ __forceinline__ bool range_maybe_donate(const LBArgs& lb, unsigned long long* range, int root,
                                                    int* donations_left, long long task_start, int* busy, int& ob,
-                                                   int& oe) {
+                                                   int& oe, int cost_tail = 0) {
   if (lb.hungry_trigger <= 0) return false;
   if (*reinterpret_cast<volatile int*>(donations_left) <= 0) return false;
   if (vload(&lb.ctr->hungry) < lb.hungry_trigger) return false;
@@ -238,7 +241,15 @@ __device__ __forceinline__ bool range_maybe_donate(const LBArgs& lb, unsigned lo
   while (true) {
     const int next = (int)(unsigned)cur, end = (int)(unsigned)(cur >> 32);
     if (end - next < 2) break;
-    const int mid = next + (end - next + 1) / 2;
+    int mid = next + (end - next + 1) / 2;
+    if (cost_tail > 0) {
+      // item i costs about (cost_tail - i): split where the remaining cost halves
+      const double a = (double)(cost_tail - next) + 0.5;
+      const double total = 0.5 * (double)(end - next) * (double)((cost_tail - next) + (cost_tail - end + 1));
+      const double disc = a * a - total;
+      const int x = (int)(a - sqrt(disc > 0 ? disc : 0.0) + 0.5);
+      mid = next + max(1, min(end - next - 1, x));
+    }
     const unsigned long long prev = atomicCAS(range, cur, pack_range(next, mid));
     if (prev != cur) {
       cur = prev;

@@ -174,7 +174,7 @@ __global__ void __launch_bounds__(32 * MOTIF_WARPS) motif_kernel(MotifArgs a) {
           it = range_take(&sw->range);
           int ob = 0, oe = 0;
           if (it >= 0 &&
-              range_maybe_donate(a.lb, &sw->range, v0, &sw->donations_left, t_start, &sw->busy, ob, oe)) {
+              range_maybe_donate(a.lb, &sw->range, v0, &sw->donations_left, t_start, &sw->busy, ob, oe, n0)) {
             // lane 0 is the only taker, so the split can be undone
             const unsigned long long cur = *reinterpret_cast<volatile unsigned long long*>(&sw->range);
             sw->range = (cur & 0xffffffffull) | ((unsigned long long)(unsigned)oe << 32);

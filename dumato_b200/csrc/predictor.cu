@@ -3,8 +3,8 @@
 // A small MLP (8 features -> 32 -> 32 -> 1, FP32, ReLU) predicts log(1 + subtree size) of a
 // root task, where the subtree size is the number of subgraphs the task counts (the log the
 // plain engine writes through dm_opts.subtree_counts). Training, gradients and inference
-// are this file's own CUDA kernels: a per-sample forward/backward with shared-memory
-// gradient accumulation, and an Adam step per parameter.
+// are this file's own CUDA kernels: a per-sample forward/backward whose activations stay in
+// shared memory, a per-parameter reduction over each block's samples, and an Adam step.
 //
 // Features of root v for a k query (all FP32):
 //   f0 log1p(deg v)            f1 log1p(core number of v)
@@ -77,72 +77,92 @@ __global__ void mlp_forward_kernel(const float* __restrict__ P, const float* __r
   y[s] = out;
 }
 
-// Gradients of mean squared error over the samples idx[0..n) (or 0..n when idx is null);
-// grad must be zeroed by the caller; loss_sum receives sum of squared errors.
-__global__ void mlp_backward_kernel(const float* __restrict__ P, const float* __restrict__ X,
-                                    const float* __restrict__ T, const int* __restrict__ idx, int n, float inv_n,
-                                    float* __restrict__ grad, float* __restrict__ loss_sum) {
-  __shared__ float sp[MLP_NP];
-  __shared__ float sg[MLP_NP];
-  for (int i = threadIdx.x; i < MLP_NP; i += blockDim.x) {
-    sp[i] = P[i];
-    sg[i] = 0.f;
-  }
+// Gradients of mean squared error over the samples idx[0..n) (or 0..n when idx is null).
+// One block takes TB samples: each thread runs one sample forward and back to the
+// pre-activation gradients, keeping inputs, activations and those gradients in shared
+// memory; then the block reduces every parameter's gradient over its samples and adds it
+// to `grad` (zeroed by the caller) with one atomic per parameter. loss_sum receives the sum
+// of squared errors.
+constexpr int TB = 128;
+constexpr int ROW = MLP_F + 4 * MLP_H + 1;  // x | h1 | h2 | dz1 | dz2 | dy
+
+__global__ void __launch_bounds__(TB) mlp_backward_kernel(const float* __restrict__ P, const float* __restrict__ X,
+                                                          const float* __restrict__ T, const int* __restrict__ idx,
+                                                          int n, float inv_n, float* __restrict__ grad,
+                                                          float* __restrict__ loss_sum) {
+  extern __shared__ float sm[];
+  float* sp = sm;               // MLP_NP
+  float* rows = sm + MLP_NP + 3;  // TB x ROW
+  for (int i = threadIdx.x; i < MLP_NP; i += blockDim.x) sp[i] = P[i];
   __syncthreads();
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int t = blockIdx.x * TB + threadIdx.x;
+  float* r = rows + threadIdx.x * ROW;
+  float* rx = r;
+  float* rh1 = r + MLP_F;
+  float* rh2 = rh1 + MLP_H;
+  float* rd1 = rh2 + MLP_H;
+  float* rd2 = rd1 + MLP_H;
+  float sq = 0.f;
   if (t < n) {
     const int s = idx ? idx[t] : t;
-    float x[MLP_F], h1[MLP_H], h2[MLP_H];
 #pragma unroll
-    for (int f = 0; f < MLP_F; ++f) x[f] = X[(size_t)s * MLP_F + f];
-#pragma unroll
+    for (int f = 0; f < MLP_F; ++f) rx[f] = X[(size_t)s * MLP_F + f];
     for (int h = 0; h < MLP_H; ++h) {
       float a = sp[OFF_B1 + h];
 #pragma unroll
-      for (int f = 0; f < MLP_F; ++f) a = fmaf(sp[OFF_W1 + h * MLP_F + f], x[f], a);
-      h1[h] = fmaxf(a, 0.f);
+      for (int f = 0; f < MLP_F; ++f) a = fmaf(sp[OFF_W1 + h * MLP_F + f], rx[f], a);
+      rh1[h] = fmaxf(a, 0.f);
     }
     float out = sp[OFF_B3];
     for (int h = 0; h < MLP_H; ++h) {
       float a = sp[OFF_B2 + h];
-#pragma unroll
-      for (int j = 0; j < MLP_H; ++j) a = fmaf(sp[OFF_W2 + h * MLP_H + j], h1[j], a);
-      h2[h] = fmaxf(a, 0.f);
-      out = fmaf(sp[OFF_W3 + h], h2[h], out);
+      for (int j = 0; j < MLP_H; ++j) a = fmaf(sp[OFF_W2 + h * MLP_H + j], rh1[j], a);
+      rh2[h] = fmaxf(a, 0.f);
+      out = fmaf(sp[OFF_W3 + h], rh2[h], out);
     }
     const float err = out - T[s];
-    atomicAdd(loss_sum, err * err);
+    sq = err * err;
     const float dy = 2.f * err * inv_n;
-    atomicAdd(&sg[OFF_B3], dy);
-    float dh1[MLP_H];
-#pragma unroll
-    for (int j = 0; j < MLP_H; ++j) dh1[j] = 0.f;
-    for (int h = 0; h < MLP_H; ++h) {
-      atomicAdd(&sg[OFF_W3 + h], dy * h2[h]);
-      const float dz2 = h2[h] > 0.f ? dy * sp[OFF_W3 + h] : 0.f;
-      if (dz2 != 0.f) {
-        atomicAdd(&sg[OFF_B2 + h], dz2);
-#pragma unroll
-        for (int j = 0; j < MLP_H; ++j) {
-          atomicAdd(&sg[OFF_W2 + h * MLP_H + j], dz2 * h1[j]);
-          dh1[j] = fmaf(dz2, sp[OFF_W2 + h * MLP_H + j], dh1[j]);
-        }
-      }
-    }
-#pragma unroll
+    r[ROW - 1] = dy;
+    for (int h = 0; h < MLP_H; ++h) rd2[h] = rh2[h] > 0.f ? dy * sp[OFF_W3 + h] : 0.f;
     for (int j = 0; j < MLP_H; ++j) {
-      const float dz1 = h1[j] > 0.f ? dh1[j] : 0.f;
-      if (dz1 != 0.f) {
-        atomicAdd(&sg[OFF_B1 + j], dz1);
-#pragma unroll
-        for (int f = 0; f < MLP_F; ++f) atomicAdd(&sg[OFF_W1 + j * MLP_F + f], dz1 * x[f]);
-      }
+      float a = 0.f;
+      for (int h = 0; h < MLP_H; ++h) a = fmaf(rd2[h], sp[OFF_W2 + h * MLP_H + j], a);
+      rd1[j] = rh1[j] > 0.f ? a : 0.f;
     }
+  } else {
+    for (int i = 0; i < ROW; ++i) r[i] = 0.f;
   }
+  for (int o = 16; o > 0; o >>= 1) sq += __shfl_xor_sync(0xffffffffu, sq, o);
+  if ((threadIdx.x & 31) == 0 && sq != 0.f) atomicAdd(loss_sum, sq);
   __syncthreads();
-  for (int i = threadIdx.x; i < MLP_NP; i += blockDim.x)
-    if (sg[i] != 0.f) atomicAdd(grad + i, sg[i]);
+  // per-parameter reductions over the block's samples
+  for (int i = threadIdx.x; i < MLP_NP; i += blockDim.x) {
+    float acc = 0.f;
+    if (i < OFF_B1) {  // W1[h][f] = sum dz1[h] x[f]
+      const int h = i / MLP_F, f = i % MLP_F;
+      for (int q = 0; q < TB; ++q) acc = fmaf(rows[q * ROW + MLP_F + 2 * MLP_H + h], rows[q * ROW + f], acc);
+    } else if (i < OFF_W2) {  // b1[h] = sum dz1[h]
+      const int h = i - OFF_B1;
+      for (int q = 0; q < TB; ++q) acc += rows[q * ROW + MLP_F + 2 * MLP_H + h];
+    } else if (i < OFF_B2) {  // W2[h][j] = sum dz2[h] h1[j]
+      const int h = (i - OFF_W2) / MLP_H, j = (i - OFF_W2) % MLP_H;
+      for (int q = 0; q < TB; ++q)
+        acc = fmaf(rows[q * ROW + MLP_F + 3 * MLP_H + h], rows[q * ROW + MLP_F + j], acc);
+    } else if (i < OFF_W3) {  // b2[h] = sum dz2[h]
+      const int h = i - OFF_B2;
+      for (int q = 0; q < TB; ++q) acc += rows[q * ROW + MLP_F + 3 * MLP_H + h];
+    } else if (i < OFF_B3) {  // W3[h] = sum dy h2[h]
+      const int h = i - OFF_W3;
+      for (int q = 0; q < TB; ++q) acc = fmaf(rows[q * ROW + ROW - 1], rows[q * ROW + MLP_F + MLP_H + h], acc);
+    } else {  // b3 = sum dy
+      for (int q = 0; q < TB; ++q) acc += rows[q * ROW + ROW - 1];
+    }
+    if (acc != 0.f) atomicAdd(grad + i, acc);
+  }
 }
+
+constexpr size_t BACKWARD_SMEM = sizeof(float) * (MLP_NP + 3 + TB * ROW);
 
 __global__ void adam_kernel(float* __restrict__ P, const float* __restrict__ g, float* __restrict__ m,
                             float* __restrict__ v, float lr, float b1, float b2, float eps, float c1, float c2) {
@@ -432,7 +452,9 @@ int dm_predictor_gradients(const dm_predictor* p, const float* X, const float* T
   cudaMemcpy(dT, T, sizeof(float) * n, cudaMemcpyHostToDevice);
   cudaMemset(dG, 0, sizeof(float) * MLP_NP);
   cudaMemset(dL, 0, sizeof(float));
-  mlp_backward_kernel<<<(unsigned)((n + 127) / 128), 128>>>(dP, dX, dT, nullptr, (int)n, 1.f / (float)n, dG, dL);
+  cudaFuncSetAttribute(mlp_backward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)BACKWARD_SMEM);
+  mlp_backward_kernel<<<(unsigned)((n + TB - 1) / TB), TB, BACKWARD_SMEM>>>(dP, dX, dT, nullptr, (int)n,
+                                                                          1.f / (float)n, dG, dL);
   cudaError_t e = cudaGetLastError();
   if (e == cudaSuccess) e = cudaMemcpy(grad, dG, sizeof(float) * MLP_NP, cudaMemcpyDeviceToHost);
   float ls = 0;
@@ -470,6 +492,7 @@ int dm_predictor_train(dm_predictor* p, const float* X, const float* T, int64_t 
   cudaMemcpy(dV, p->adam_v.data(), sizeof(float) * MLP_NP, cudaMemcpyHostToDevice);
   cudaMemcpy(dX, X, sizeof(float) * n * MLP_F, cudaMemcpyHostToDevice);
   cudaMemcpy(dT, T, sizeof(float) * n, cudaMemcpyHostToDevice);
+  cudaFuncSetAttribute(mlp_backward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)BACKWARD_SMEM);
   std::vector<int> idx(n);
   std::iota(idx.begin(), idx.end(), 0);
   uint64_t s = p->seed ^ 0x5DEECE66Dull;
@@ -485,7 +508,8 @@ int dm_predictor_train(dm_predictor* p, const float* X, const float* T, int64_t 
     for (int64_t off = 0; off < n; off += batch) {
       const int bn = (int)std::min<int64_t>(batch, n - off);
       cudaMemsetAsync(dG, 0, sizeof(float) * MLP_NP);
-      mlp_backward_kernel<<<(bn + 127) / 128, 128>>>(dP, dX, dT, dIdx + off, bn, 1.f / (float)bn, dG, dL);
+      mlp_backward_kernel<<<(bn + TB - 1) / TB, TB, BACKWARD_SMEM>>>(dP, dX, dT, dIdx + off, bn, 1.f / (float)bn,
+                                                                     dG, dL);
       ++p->steps;
       const float c1 = 1.f - std::pow(b1, (float)p->steps), c2 = 1.f - std::pow(b2, (float)p->steps);
       adam_kernel<<<(MLP_NP + 255) / 256, 256>>>(dP, dG, dM, dV, lr, b1, b2, 1e-8f, c1, c2);

@@ -121,6 +121,7 @@ typedef struct dm_stats {
   int32_t block;               /* threads per CTA */
   int32_t kernel_launches;     /* kernels of this library launched for the call */
   int32_t reserved;
+  double idle_warp_fraction;   /* time warps waited for work / (warps x kernel time) */
 } dm_stats;
 
 /* ---- version / errors ---- */
