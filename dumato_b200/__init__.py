@@ -69,7 +69,8 @@ class _Stats(ctypes.Structure):
                 ("donations", ctypes.c_uint64), ("idle_polls", ctypes.c_uint64), ("nodes", ctypes.c_uint64),
                 ("mode_used", ctypes.c_int32), ("vwarp_used", ctypes.c_int32), ("grid", ctypes.c_int32),
                 ("block", ctypes.c_int32), ("kernel_launches", ctypes.c_int32), ("reserved", ctypes.c_int32),
-                ("idle_warp_fraction", ctypes.c_double)]
+                ("idle_warp_fraction", ctypes.c_double), ("max_task_ms", ctypes.c_double),
+                ("max_task_root", ctypes.c_int32), ("reserved2", ctypes.c_int32)]
 
 
 _P = ctypes.c_void_p
@@ -422,11 +423,14 @@ class Stats:
     block: int = 0
     kernel_launches: int = 0
     idle_warp_fraction: float = 0.0
+    max_task_ms: float = 0.0
+    max_task_root: int = -1
 
     @classmethod
     def from_c(cls, s: _Stats) -> "Stats":
         return cls(s.kernel_ms, s.prep_ms, s.tasks, s.donations, s.idle_polls, s.nodes, s.mode_used,
-                   s.vwarp_used, s.grid, s.block, s.kernel_launches, s.idle_warp_fraction)
+                   s.vwarp_used, s.grid, s.block, s.kernel_launches, s.idle_warp_fraction, s.max_task_ms,
+                   s.max_task_root)
 
 
 def clique_work_model(g: Graph, k: int) -> tuple[int, int]:

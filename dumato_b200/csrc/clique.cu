@@ -455,6 +455,7 @@ __global__ void __launch_bounds__(256) clique_kernel(CliqueArgs a) {
       int bb = b, ee = e;
       if (!donated && a.parts) part_bounds(__ldg(a.parts + first + ti), bb, ee);
       ++ntasks;
+      const long long t_task = global_ns();
       unsigned long long task_cnt = 0;
       const int d = __ldg(a.g.deg + root);
       if (e >= 0 && b >= e) {
@@ -481,6 +482,7 @@ __global__ void __launch_bounds__(256) clique_kernel(CliqueArgs a) {
         if (lane == 0 && tsum) atomicAdd(a.per_root + root, tsum);
       }
       __syncwarp();
+      if (lane == 0) lb_task_time(a.lb, t_task, root);
     }
     if (lane == 0) lb_done(a.lb, count);
   }

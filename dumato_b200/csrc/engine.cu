@@ -78,6 +78,16 @@ struct DeviceSlot {
   // motif roots (vertices with a neighbour above them) by descending upper degree
   int32_t* d_up_order = nullptr;
   int n_up = 0;
+  // last learned schedule per engine (0 = motifs, 1 = cliques), reused while its key holds
+  struct Learned {
+    bool valid = false;
+    int k = 0, world = 1, rank = 0;
+    uint64_t uid = 0, version = 0;
+    int32_t* d_roots = nullptr;
+    int32_t* d_parts = nullptr;
+    size_t cap = 0;
+    int n = 0, max_d = 0;
+  } learned[2];
 };
 
 static std::mutex g_dev_mu;
@@ -224,6 +234,10 @@ void release_device_graphs(dm_graph* g) {
       cudaFree(s->ws.d_parts);
       cudaFree(s->d_deg_order);
       cudaFree(s->d_up_order);
+      for (auto& l : s->learned) {
+        cudaFree(l.d_roots);
+        cudaFree(l.d_parts);
+      }
       if (s->ws.ev0) cudaEventDestroy(s->ws.ev0);
       if (s->ws.ev1) cudaEventDestroy(s->ws.ev1);
       if (s->ws.k0) cudaEventDestroy(s->ws.k0);
@@ -288,6 +302,53 @@ static int ensure_deg_order(dm_graph* g, DeviceSlot* s, cudaStream_t st) {
 int predictor_schedule(const void* pv, dm_graph* g, int k, bool clique, int total_warps, std::vector<int32_t>& roots,
                        std::vector<int32_t>& parts);
 int ensure_features(dm_graph* g, bool clique);
+void predictor_key(const void* pv, uint64_t* uid, uint64_t* version);
+
+// Looks up (or fills) the cached learned schedule of this graph, device and engine.
+static bool learned_cached(DeviceSlot* s, int eng, int k, const dm_opts* o, const int32_t** roots,
+                           const int32_t** parts, int* n, int* max_d) {
+  uint64_t uid, ver;
+  predictor_key(o->predictor, &uid, &ver);
+  auto& l = s->learned[eng];
+  const int world = o->world_size > 1 ? o->world_size : 1, rank = world > 1 ? o->rank : 0;
+  if (!(l.valid && l.k == k && l.uid == uid && l.version == ver && l.world == world && l.rank == rank)) return false;
+  *roots = l.d_roots;
+  *parts = l.d_parts;
+  *n = l.n;
+  *max_d = l.max_d;
+  return true;
+}
+
+static int learned_store(DeviceSlot* s, int eng, int k, const dm_opts* o, const std::vector<int32_t>& roots,
+                         const std::vector<int32_t>& parts, int max_d, cudaStream_t st, const int32_t** d_roots,
+                         const int32_t** d_parts) {
+  auto& l = s->learned[eng];
+  l.valid = false;
+  const size_t n = std::max<size_t>(roots.size(), 1);
+  if (l.cap < n) {
+    cudaFree(l.d_roots);
+    cudaFree(l.d_parts);
+    l.d_roots = l.d_parts = nullptr;
+    l.cap = 0;
+    DM_CUDA(cudaMalloc(&l.d_roots, sizeof(int32_t) * n));
+    DM_CUDA(cudaMalloc(&l.d_parts, sizeof(int32_t) * n));
+    l.cap = n;
+  }
+  if (!roots.empty()) {
+    DM_CUDA(cudaMemcpyAsync(l.d_roots, roots.data(), sizeof(int32_t) * roots.size(), cudaMemcpyHostToDevice, st));
+    DM_CUDA(cudaMemcpyAsync(l.d_parts, parts.data(), sizeof(int32_t) * parts.size(), cudaMemcpyHostToDevice, st));
+  }
+  predictor_key(o->predictor, &l.uid, &l.version);
+  l.k = k;
+  l.world = o->world_size > 1 ? o->world_size : 1;
+  l.rank = l.world > 1 ? o->rank : 0;
+  l.n = (int)roots.size();
+  l.max_d = max_d;
+  l.valid = true;
+  *d_roots = l.d_roots;
+  *d_parts = l.d_parts;
+  return DM_OK;
+}
 
 static int order_roots(dm_graph* g, const dm_opts* o, int k, bool clique, int total_warps,
                        std::vector<int32_t>& roots, std::vector<int32_t>& parts) {
@@ -386,6 +447,10 @@ int dm_count_cliques(dm_graph* g, int32_t k, const dm_opts* o, uint64_t* count, 
     n_roots = need <= g->max_out_degree ? (int)s->cnt_ge[need] : 0;
     d_roots = s->d_deg_order;
     max_d = n_roots ? (int)(g->orow[s->deg_order[0] + 1] - g->orow[s->deg_order[0]]) : 0;
+  }
+  const int32_t* d_parts = nullptr;
+  if (d_roots) {
+  } else if (sched == DM_SCHED_LEARNED && learned_cached(s, 1, k, o, &d_roots, &d_parts, &n_roots, &max_d)) {
   } else {
     roots.reserve(g->n);
     for (int32_t r = 0; r < g->n; ++r)
@@ -393,9 +458,12 @@ int dm_count_cliques(dm_graph* g, int32_t k, const dm_opts* o, uint64_t* count, 
     if ((rc = order_roots(g, o, k, true, ctx.num_sms * 32, roots, parts))) return rc;
     for (int32_t r : roots) max_d = std::max(max_d, (int)(g->orow[r + 1] - g->orow[r]));
     n_roots = (int)roots.size();
+    if (sched == DM_SCHED_LEARNED) {
+      if ((rc = learned_store(s, 1, k, o, roots, parts, max_d, ctx.stream, &d_roots, &d_parts))) return rc;
+    } else if ((rc = upload_parts(ws, parts, ctx.stream, &d_parts))) {
+      return rc;
+    }
   }
-  const int32_t* d_parts = nullptr;
-  if ((rc = upload_parts(ws, parts, ctx.stream, &d_parts))) return rc;
   const int mode = o ? o->mode : DM_MODE_AUTO;
   CliqueLaunch L;
   L.k = k;
@@ -483,6 +551,8 @@ int dm_count_cliques(dm_graph* g, int32_t k, const dm_opts* o, uint64_t* count, 
     st->kernel_launches = ctx.launches;
     const double warp_ns = (double)grid * 8.0 * (double)kms * 1e6;
     st->idle_warp_fraction = warp_ns > 0 ? std::min(1.0, (double)h.hungry_ns / warp_ns) : 0.0;
+    st->max_task_ms = (double)h.max_task_ns * 1e-6;
+    st->max_task_root = h.max_task_root;
   }
   return DM_OK;
 }
@@ -530,21 +600,29 @@ int dm_count_motifs(dm_graph* g, int32_t k, const dm_dictionary* dict, const dm_
     s->n_up = (int)order.size();
   }
   std::vector<int32_t> roots, parts;
+  const int32_t* d_parts_cached = nullptr;
+  int max_d_unused = 0;
   if (sched == DM_SCHED_PLAIN && world == 1) {
     d_roots = s->d_up_order;
     n_roots = s->n_up;
+  } else if (sched == DM_SCHED_LEARNED && learned_cached(s, 0, k, o, &d_roots, &d_parts_cached, &n_roots,
+                                                         &max_d_unused)) {
   } else {
     for (int32_t v = 0; v < g->n; ++v)
       if (upper(v) > 0) roots.push_back(v);
     if ((rc = order_roots(g, o, k, false, ctx.num_sms * 32, roots, parts))) return rc;
     n_roots = (int)roots.size();
-    if ((rc = ensure_ws_bytes(reinterpret_cast<void**>(&ws.d_tasks), &ws.tasks_cap,
-                              sizeof(int32_t) * (roots.size() + 1))))
-      return rc;
-    if (!roots.empty())
-      DM_CUDA(cudaMemcpyAsync(ws.d_tasks, roots.data(), sizeof(int32_t) * roots.size(), cudaMemcpyHostToDevice,
-                              ctx.stream));
-    d_roots = ws.d_tasks;
+    if (sched == DM_SCHED_LEARNED) {
+      if ((rc = learned_store(s, 0, k, o, roots, parts, 0, ctx.stream, &d_roots, &d_parts_cached))) return rc;
+    } else {
+      if ((rc = ensure_ws_bytes(reinterpret_cast<void**>(&ws.d_tasks), &ws.tasks_cap,
+                                sizeof(int32_t) * (roots.size() + 1))))
+        return rc;
+      if (!roots.empty())
+        DM_CUDA(cudaMemcpyAsync(ws.d_tasks, roots.data(), sizeof(int32_t) * roots.size(), cudaMemcpyHostToDevice,
+                                ctx.stream));
+      d_roots = ws.d_tasks;
+    }
   }
   // dictionary table
   if (ws.q2c_uid != dict->uid) {
@@ -572,8 +650,8 @@ int dm_count_motifs(dm_graph* g, int32_t k, const dm_dictionary* dict, const dm_
     DM_CUDA(cudaMemsetAsync(ws.d_per_root, 0, sizeof(unsigned long long) * std::max(g->n, 1), ctx.stream));
   }
   if ((rc = init_counters(ws, n_roots, ctx.stream))) return rc;
-  const int32_t* d_parts = nullptr;
-  if ((rc = upload_parts(ws, parts, ctx.stream, &d_parts))) return rc;
+  const int32_t* d_parts = d_parts_cached;
+  if (!d_parts && (rc = upload_parts(ws, parts, ctx.stream, &d_parts))) return rc;
   MotifLaunch L;
   L.parts = d_parts;
   L.g = GraphView{s->dg.d_row, s->dg.d_deg, s->dg.d_adj, g->n};
@@ -627,6 +705,8 @@ int dm_count_motifs(dm_graph* g, int32_t k, const dm_dictionary* dict, const dm_
     st->kernel_launches = ctx.launches;
     const double warp_ns = (double)grid * 8.0 * (double)kms * 1e6;
     st->idle_warp_fraction = warp_ns > 0 ? std::min(1.0, (double)h.hungry_ns / warp_ns) : 0.0;
+    st->max_task_ms = (double)h.max_task_ns * 1e-6;
+    st->max_task_root = h.max_task_root;
   }
   return DM_OK;
 }

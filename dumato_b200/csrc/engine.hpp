@@ -28,6 +28,8 @@ struct alignas(128) DevCounters {
   unsigned long long donations;  // donated ranges
   unsigned long long idle_polls; // polls of the donation queue by hungry warps
   unsigned long long hungry_ns;  // time warps spent waiting for work, summed over warps
+  unsigned long long max_task_ns;  // longest single task
+  int max_task_root;             // its root (best effort under races)
   int err;                       // first error code raised by a kernel (0 = none)
   int err_info;
 };

@@ -182,6 +182,13 @@ static __device__ __noinline__ bool lb_next(const LBArgs& lb, int n_roots, int t
   return got;
 }
 
+// Records a finished task's duration (lane 0).
+__device__ __forceinline__ void lb_task_time(const LBArgs& lb, long long t_start, int root) {
+  const unsigned long long dur = (unsigned long long)(global_ns() - t_start);
+  const unsigned long long old = atomicMax(&lb.ctr->max_task_ns, dur);
+  if (dur > old) lb.ctr->max_task_root = root;
+}
+
 __device__ __forceinline__ void lb_done(const LBArgs& lb, int count) {
   __threadfence();
   atomicSub(&lb.ctr->pending, count);

@@ -323,6 +323,7 @@ __global__ void __launch_bounds__(32 * MOTIF_WARPS) motif_kernel(MotifArgs a) {
         if (lane == 0 && tsum) atomicAdd(a.per_root + v0, tsum);
       }
       __syncwarp();
+      if (lane == 0) lb_task_time(a.lb, t_start, v0);
     }
     if (lane == 0) lb_done(a.lb, count);
   }

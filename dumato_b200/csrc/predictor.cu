@@ -21,6 +21,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -42,6 +43,8 @@ constexpr int MLP_NP = OFF_B3 + 1;              // 1377
 
 struct dm_predictor {
   int device = -1;
+  uint64_t uid = 0;           // identity for schedule caches
+  uint64_t version = 0;       // bumped whenever the parameters change
   std::vector<float> params;  // host copy (authoritative between calls)
   uint64_t seed = 0;
   int steps = 0;
@@ -49,6 +52,15 @@ struct dm_predictor {
 };
 
 namespace dmb {
+
+static std::atomic<uint64_t> g_pred_uid{1};
+
+// (identity, parameter version) of a predictor, the key of cached learned schedules.
+void predictor_key(const void* pv, uint64_t* uid, uint64_t* version) {
+  const dm_predictor* p = reinterpret_cast<const dm_predictor*>(pv);
+  *uid = p->uid;
+  *version = p->version;
+}
 
 __global__ void mlp_forward_kernel(const float* __restrict__ P, const float* __restrict__ X, int n,
                                    float* __restrict__ y) {
@@ -381,6 +393,7 @@ extern "C" {
 int dm_predictor_create(uint64_t seed, dm_predictor** out) {
   if (!out) return fail(DM_EINVAL, "dm_predictor_create: null argument");
   auto* p = new dm_predictor();
+  p->uid = g_pred_uid++;
   p->seed = seed;
   p->params.assign(MLP_NP, 0.f);
   // He-uniform initialisation from a splitmix stream
@@ -414,6 +427,7 @@ int dm_predictor_get_params(const dm_predictor* p, float* params) {
 int dm_predictor_set_params(dm_predictor* p, const float* params) {
   if (!p || !params) return fail(DM_EINVAL, "dm_predictor_set_params: null argument");
   std::memcpy(p->params.data(), params, sizeof(float) * MLP_NP);
+  ++p->version;
   return DM_OK;
 }
 
@@ -520,6 +534,7 @@ int dm_predictor_train(dm_predictor* p, const float* X, const float* T, int64_t 
   }
   cudaError_t e = cudaGetLastError();
   if (e == cudaSuccess) e = cudaMemcpy(p->params.data(), dP, sizeof(float) * MLP_NP, cudaMemcpyDeviceToHost);
+  ++p->version;
   if (e == cudaSuccess) e = cudaMemcpy(p->adam_m.data(), dM, sizeof(float) * MLP_NP, cudaMemcpyDeviceToHost);
   if (e == cudaSuccess) e = cudaMemcpy(p->adam_v.data(), dV, sizeof(float) * MLP_NP, cudaMemcpyDeviceToHost);
   cudaFree(dP);

@@ -122,6 +122,9 @@ typedef struct dm_stats {
   int32_t kernel_launches;     /* kernels of this library launched for the call */
   int32_t reserved;
   double idle_warp_fraction;   /* time warps waited for work / (warps x kernel time) */
+  double max_task_ms;          /* longest single task (root or donated range) */
+  int32_t max_task_root;       /* its root (cliques: rank space; motifs: vertex id) */
+  int32_t reserved2;
 } dm_stats;
 
 /* ---- version / errors ---- */
