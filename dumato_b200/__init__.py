@@ -61,7 +61,8 @@ class _Opts(ctypes.Structure):
                 ("donations_per_warp", ctypes.c_int32), ("threshold", ctypes.c_int32),
                 ("vwarp", ctypes.c_int32), ("mode", ctypes.c_int32), ("scheduler", ctypes.c_int32),
                 ("rank", ctypes.c_int32), ("world_size", ctypes.c_int32), ("timeout_ms", ctypes.c_int32),
-                ("predictor", ctypes.c_void_p), ("subtree_counts", ctypes.c_void_p)]
+                ("predictor", ctypes.c_void_p), ("subtree_counts", ctypes.c_void_p),
+                ("test_flags", ctypes.c_int32), ("reserved", ctypes.c_int32)]
 
 
 class _Stats(ctypes.Structure):
@@ -95,6 +96,8 @@ _SIGNATURES = {
     "dm_dictionary_connected": (ctypes.c_int, [_P, _P]),
     "dm_dictionary_free": (None, [_P]),
     "dm_clique_work_model": (ctypes.c_int, [_P, ctypes.c_int32, _P, _P]),
+    "dm_plan_roots": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(_Opts), _P, _P, ctypes.c_int64,
+                                     ctypes.POINTER(ctypes.c_int64)]),
     "dm_predictor_create": (ctypes.c_int, [ctypes.c_uint64, ctypes.POINTER(_P)]),
     "dm_predictor_free": (None, [_P]),
     "dm_predictor_num_params": (ctypes.c_int, []),
@@ -395,6 +398,7 @@ class Options:
     timeout_ms: int = 0
     predictor: Optional[int] = None
     subtree_counts: Optional[np.ndarray] = None   # uint64[n_vertices], filled per root
+    test_flags: int = 0
 
     def to_c(self) -> _Opts:
         st = None
@@ -406,7 +410,8 @@ class Options:
                      threads=self.threads, block_size=self.block_size,
                      donations_per_warp=self.donations_per_warp, threshold=self.threshold, vwarp=self.vwarp,
                      mode=self.mode, scheduler=self.scheduler, rank=self.rank, world_size=self.world_size,
-                     timeout_ms=self.timeout_ms, predictor=self.predictor, subtree_counts=st)
+                     timeout_ms=self.timeout_ms, predictor=self.predictor, subtree_counts=st,
+                     test_flags=self.test_flags)
 
 
 @dataclass
@@ -440,6 +445,21 @@ def clique_work_model(g: Graph, k: int) -> tuple[int, int]:
     b = ctypes.c_uint64()
     _check(lib().dm_clique_work_model(g.handle, int(k), ctypes.byref(n), ctypes.byref(b)))
     return n.value, b.value
+
+
+TEST_STALL_AT_EXIT = 1
+
+
+def plan_roots(g: Graph, k: int, clique: bool = True, opts: Optional[Options] = None) -> tuple[np.ndarray, np.ndarray]:
+    """The ordered root tasks (original ids, part words) this shard would run (host only)."""
+    o = (opts or Options()).to_c()
+    n = ctypes.c_int64()
+    _check(lib().dm_plan_roots(g.handle, int(k), 1 if clique else 0, ctypes.byref(o), None, None, 0, ctypes.byref(n)))
+    roots = np.empty(n.value, np.int32)
+    parts = np.empty(n.value, np.int32)
+    _check(lib().dm_plan_roots(g.handle, int(k), 1 if clique else 0, ctypes.byref(o), _ptr(roots), _ptr(parts),
+                               n.value, ctypes.byref(n)))
+    return roots, parts
 
 
 def count_cliques(g: Graph, k: int, opts: Optional[Options] = None) -> tuple[int, Stats]:

@@ -130,6 +130,7 @@ static int select_device(const dm_opts* o, LaunchCtx& ctx) {
     ctx.vwarp = o->vwarp;
     ctx.threshold = o->threshold > 0 ? o->threshold : 0;
     ctx.donations_per_warp = o->donations_per_warp > 0 ? o->donations_per_warp : 16;
+    ctx.test_stall = (o->test_flags & DM_TEST_STALL_AT_EXIT) ? 1 : 0;
   }
   return DM_OK;
 }
@@ -707,6 +708,41 @@ int dm_count_motifs(dm_graph* g, int32_t k, const dm_dictionary* dict, const dm_
     st->idle_warp_fraction = warp_ns > 0 ? std::min(1.0, (double)h.hungry_ns / warp_ns) : 0.0;
     st->max_task_ms = (double)h.max_task_ns * 1e-6;
     st->max_task_root = h.max_task_root;
+  }
+  return DM_OK;
+}
+
+int dm_plan_roots(dm_graph* g, int32_t k, int32_t clique, const dm_opts* o, int32_t* out_roots, int32_t* out_parts,
+                  int64_t cap, int64_t* n_out) {
+  if (!g || !n_out || (cap > 0 && (!out_roots || !out_parts))) return fail(DM_EINVAL, "dm_plan_roots: bad arguments");
+  if (k < 2 || k > 12 || (!clique && (k < 3 || k > 7))) return fail(DM_EINVAL, "dm_plan_roots: k out of range");
+  int rc = check_opts(o);
+  if (rc) return rc;
+  if (o && o->scheduler == DM_SCHED_LEARNED && (rc = ensure_features(g, clique != 0))) return rc;
+  std::lock_guard<std::mutex> lk(g->mu);
+  ensure_oriented(g);
+  std::vector<int32_t> roots, parts;
+  if (clique) {
+    for (int32_t r = 0; r < g->n; ++r)
+      if (g->orow[r + 1] - g->orow[r] >= k - 1) roots.push_back(r);
+  } else {
+    for (int32_t v = 0; v < g->n; ++v) {
+      const int32_t* b = g->adj.data() + g->row[v];
+      const int32_t* e = g->adj.data() + g->row[v + 1];
+      if (e - std::upper_bound(b, e, v) > 0) roots.push_back(v);
+    }
+  }
+  int sms = 148;
+  if ((rc = order_roots(g, o, k, clique != 0, sms * 32, roots, parts))) return rc;
+  if (clique) {
+    std::vector<int32_t> inv(g->n);
+    for (int32_t v = 0; v < g->n; ++v) inv[g->rank[v]] = v;
+    for (auto& r : roots) r = inv[r];
+  }
+  *n_out = (int64_t)roots.size();
+  for (int64_t i = 0; i < std::min<int64_t>(cap, (int64_t)roots.size()); ++i) {
+    out_roots[i] = roots[i];
+    out_parts[i] = parts.empty() ? 0 : parts[i];
   }
   return DM_OK;
 }

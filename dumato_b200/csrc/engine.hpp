@@ -30,6 +30,7 @@ struct alignas(128) DevCounters {
   unsigned long long hungry_ns;  // time warps spent waiting for work, summed over warps
   unsigned long long max_task_ns;  // longest single task
   int max_task_root;             // its root (best effort under races)
+  int test_gate;                 // never written by the library (failure-path tests)
   int err;                       // first error code raised by a kernel (0 = none)
   int err_info;
 };
@@ -58,6 +59,7 @@ struct LaunchCtx {
   int donations_per_warp = 16;
   int arena_warps = 0;   // warps the list arena has room for
   int donate_after_us = 20;  // a task donates only after running this long
+  int test_stall = 0;        // DM_TEST_STALL_AT_EXIT
 };
 
 // Clique engine (clique.cu).

@@ -52,6 +52,7 @@ struct LBArgs {
   int max_donations;     // per task
   long long donate_after_ns;  // a task donates only after running this long
   long long timeout_ns;
+  int test_stall;             // test hook: wait at exit on a word nothing sets
 };
 
 __device__ __forceinline__ long long global_ns() {
@@ -162,6 +163,18 @@ static __device__ __noinline__ bool lb_next(const LBArgs& lb, int n_roots, int t
       break;
     }
     const int pend = vload(&c->pending);
+    if (pend <= 0 && lb.test_stall) {
+      // test hook: wait for test_gate, which nothing sets, until the bounded wait gives up
+      const long long ts = global_ns();
+      while (vload(&c->test_gate) == 0) {
+        if (global_ns() - ts > lb.timeout_ns) {
+          set_err(c, ERR_TIMEOUT);
+          break;
+        }
+        __nanosleep(2000);
+      }
+      break;
+    }
     if (pend <= 0 || vload(&c->err) != 0) break;
     const unsigned long long p = vload64(&c->progress);
     if (p != last || pend != last_pending) {

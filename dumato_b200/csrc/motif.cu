@@ -372,7 +372,8 @@ int motif_launch(const MotifLaunch& L, LaunchCtx& ctx, int* grid) {
   a.n_roots = L.n_roots;
   a.lb = LBArgs{L.ctr, reinterpret_cast<QHeader*>(L.queue),
                 reinterpret_cast<QSlot*>(reinterpret_cast<char*>(L.queue) + sizeof(QHeader)), L.qcap, 0,
-                L.max_donations, (long long)ctx.donate_after_us * 1000ll, (long long)ctx.timeout_ms * 1000000ll};
+                L.max_donations, (long long)ctx.donate_after_us * 1000ll, (long long)ctx.timeout_ms * 1000000ll,
+                ctx.test_stall};
   a.k = L.k;
   a.q2c = L.q2c;
   a.n_classes = L.n_classes;

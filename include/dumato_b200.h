@@ -106,7 +106,14 @@ typedef struct dm_opts {
   const void* predictor;       /* dm_predictor* for DM_SCHED_LEARNED, else NULL */
   uint64_t* subtree_counts;    /* optional, n_vertices entries (original ids), overwritten: the
                                   subgraphs counted under each root task (the subtree-size log) */
+  int32_t test_flags;          /* DM_TEST_* (tests of the failure paths only), else 0 */
+  int32_t reserved;
 } dm_opts;
+
+/* test_flags: every warp that finishes waits on a device word nothing sets, so the bounded
+   wait expires and the call returns DM_ETIMEOUT (exercises the timeout path without a
+   fault or a hang; use a short timeout_ms). */
+#define DM_TEST_STALL_AT_EXIT 1
 
 typedef struct dm_stats {
   double kernel_ms;            /* device time of the counting kernels (CUDA events) */
@@ -189,6 +196,13 @@ DM_API int dm_clique_work_model(dm_graph* g, int32_t k, uint64_t* nodes, uint64_
 DM_API int dm_count_cliques_noalloc(const int32_t* d_row, const int32_t* d_deg, const int32_t* d_adj,
                                     int32_t n_vertices, const int32_t* d_roots, int32_t n_roots,
                                     int32_t max_out_degree, int32_t k, uint64_t stream, uint64_t* count);
+
+/* Host-only planning: the ordered root tasks this shard (o->rank of o->world_size) would run
+   for a k query (clique != 0: cliques, else motifs), as original vertex ids with their part
+   words (p | P << 16, 0 = whole root). Writes at most cap entries and the total to *n. The
+   plain and id schedules need no device. */
+DM_API int dm_plan_roots(dm_graph* g, int32_t k, int32_t clique, const dm_opts* o, int32_t* roots, int32_t* parts,
+                         int64_t cap, int64_t* n);
 
 /* ---- learned work predictor (no counterpart in the reference) ----
    An 8 -> 32 -> 32 -> 1 FP32 MLP predicting log(1 + subtree size) of a root task, trained

@@ -45,6 +45,8 @@ def lib() -> ctypes.CDLL:
             "oracle_motifs": (ctypes.c_int, [_P, ctypes.c_int, _P, ctypes.c_int32, _P, ctypes.c_int]),
             "oracle_motifs_range": (ctypes.c_int, [_P, ctypes.c_int, _P, ctypes.c_int32, _P, ctypes.c_int32,
                                                    ctypes.c_int32, ctypes.c_int, _P]),
+            "oracle_motifs_roots": (ctypes.c_int, [_P, ctypes.c_int, _P, ctypes.c_int32, _P, _P, ctypes.c_int64,
+                                                   ctypes.c_int]),
             "oracle_motifs_brute": (ctypes.c_int, [_P, ctypes.c_int, _P, ctypes.c_int32, _P]),
         }
         for name, (res, args) in sig.items():
@@ -132,6 +134,15 @@ def motifs(g: OracleGraph, k: int, q2c: np.ndarray, n_classes: int, threads: int
     if rc != 0:
         raise RuntimeError(f"oracle_motifs failed ({rc})")
     return (hist, b.value) if with_bytes else hist
+
+
+def motifs_roots(g: OracleGraph, k: int, q2c: np.ndarray, n_classes: int, roots, threads: int = 0) -> np.ndarray:
+    q = np.ascontiguousarray(q2c, dtype=np.int32)
+    r = np.ascontiguousarray(roots, dtype=np.int32)
+    hist = np.zeros(n_classes, np.uint64)
+    if lib().oracle_motifs_roots(g.h, k, q.ctypes.data, n_classes, hist.ctypes.data, r.ctypes.data, r.size, threads):
+        raise RuntimeError("oracle_motifs_roots failed")
+    return hist
 
 
 def motifs_brute(g: OracleGraph, k: int, q2c: np.ndarray, n_classes: int) -> np.ndarray:

@@ -604,3 +604,32 @@ uint64_t oracle_clique_dfs_roots(const og_graph *g, int K, const int32_t *roots,
     if (roots[i] >= 0 && roots[i] < g->n) total += clique_root(g, roots[i], K);
   return total;
 }
+
+/* Motif counts over an explicit list of roots (shard checks). */
+int oracle_motifs_roots(const og_graph *g, int K, const int32_t *q2c, int32_t n_classes, uint64_t *hist,
+                        const int32_t *roots, int64_t n_roots, int threads) {
+  if (K < 3 || K > 7) return -2;
+  int overflow = 0;
+  int32_t cap = (int32_t)((int64_t)g->maxdeg * K + 64);
+#pragma omp parallel num_threads(resolve_threads(threads))
+  {
+    uint64_t *h = (uint64_t *)calloc((size_t)n_classes, sizeof(uint64_t));
+    motif_ws ws;
+    ws.cap = cap;
+    ws.ext = (int32_t *)malloc(sizeof(int32_t) * (size_t)cap * K);
+    ws.src = (int32_t *)malloc(sizeof(int32_t) * (size_t)cap * K);
+    int ov = 0;
+#pragma omp for schedule(dynamic, 1)
+    for (int64_t i = 0; i < n_roots; ++i)
+      if (!ov && roots[i] >= 0 && roots[i] < g->n) motif_root(g, roots[i], K, q2c, h, &ws, NULL, &ov);
+#pragma omp critical
+    {
+      for (int32_t c = 0; c < n_classes; ++c) hist[c] += h[c];
+      if (ov) overflow = 1;
+    }
+    free(h);
+    free(ws.ext);
+    free(ws.src);
+  }
+  return overflow ? -1 : 0;
+}
