@@ -455,7 +455,6 @@ __global__ void __launch_bounds__(256) clique_kernel(CliqueArgs a) {
       int bb = b, ee = e;
       if (!donated && a.parts) part_bounds(__ldg(a.parts + first + ti), bb, ee);
       ++ntasks;
-      const long long t_task = global_ns();
       unsigned long long task_cnt = 0;
       const int d = __ldg(a.g.deg + root);
       if (e >= 0 && b >= e) {
@@ -482,7 +481,6 @@ __global__ void __launch_bounds__(256) clique_kernel(CliqueArgs a) {
         if (lane == 0 && tsum) atomicAdd(a.per_root + root, tsum);
       }
       __syncwarp();
-      if (lane == 0) lb_task_time(a.lb, t_task, root);
     }
     if (lane == 0) lb_done(a.lb, count);
   }
@@ -537,9 +535,9 @@ int clique_launch(const CliqueLaunch& L, LaunchCtx& ctx, int* grid) {
   a.roots = L.roots;
   a.n_roots = L.n_roots;
   a.lb = LBArgs{L.ctr, reinterpret_cast<QHeader*>(L.queue),
-                reinterpret_cast<QSlot*>(reinterpret_cast<char*>(L.queue) + sizeof(QHeader)), L.qcap, 0,
+                reinterpret_cast<QSlot*>(reinterpret_cast<char*>(L.queue) + sizeof(QHeader) * L.nq), L.qcap, 0,
                 L.max_donations, (long long)ctx.donate_after_us * 1000ll, (long long)ctx.timeout_ms * 1000000ll,
-                ctx.test_stall};
+                ctx.test_stall, 32, L.nq};
   a.arena = L.arena;
   a.arena_dcap = L.arena_dcap;
   a.list_threshold = L.list_threshold;

@@ -45,24 +45,26 @@ struct Workspace {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, k0 = nullptr, k1 = nullptr;
 };
 
-constexpr int QUEUE_SLOTS = 1 << 16;
+constexpr int QUEUE_SHARDS = 64;
+constexpr int QUEUE_SHARD_SLOTS = 2048;
 
-__global__ void queue_init_kernel(QHeader* h, QSlot* q, int cap) {
+// Empty state: every shard's positions at 0, slot j of a shard carrying sequence j.
+__global__ void queue_init_kernel(QHeader* h, QSlot* q, int nq, int cap) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i == 0) {
-    h->write_pos = 0;
-    h->read_pos = 0;
+  if (i < nq) {
+    h[i].write_pos = 0;
+    h[i].read_pos = 0;
   }
-  if (i < cap) {
-    q[i].seq = (unsigned)i;
+  if (i < nq * cap) {
+    q[i].seq = (unsigned)(i % cap);
     q[i].root = q[i].begin = q[i].end = 0;
   }
 }
 
 static int init_queue(Workspace& ws, cudaStream_t st) {
   QHeader* h = reinterpret_cast<QHeader*>(ws.d_queue);
-  QSlot* q = reinterpret_cast<QSlot*>(reinterpret_cast<char*>(ws.d_queue) + sizeof(QHeader));
-  queue_init_kernel<<<(ws.qcap + 255) / 256, 256, 0, st>>>(h, q, ws.qcap);
+  QSlot* q = reinterpret_cast<QSlot*>(reinterpret_cast<char*>(ws.d_queue) + sizeof(QHeader) * QUEUE_SHARDS);
+  queue_init_kernel<<<(QUEUE_SHARDS * ws.qcap + 255) / 256, 256, 0, st>>>(h, q, QUEUE_SHARDS, ws.qcap);
   DM_CUDA(cudaGetLastError());
   return DM_OK;
 }
@@ -190,8 +192,9 @@ static int prepare_ws(Workspace& ws, cudaStream_t st) {
     DM_CUDA(cudaEventCreate(&ws.k1));
   }
   if (!ws.d_queue) {
-    DM_CUDA(cudaMalloc(&ws.d_queue, sizeof(QHeader) + QUEUE_SLOTS * sizeof(QSlot)));
-    ws.qcap = QUEUE_SLOTS;
+    DM_CUDA(cudaMalloc(&ws.d_queue,
+                       sizeof(QHeader) * QUEUE_SHARDS + (size_t)QUEUE_SHARDS * QUEUE_SHARD_SLOTS * sizeof(QSlot)));
+    ws.qcap = QUEUE_SHARD_SLOTS;
     int rc = init_queue(ws, st);
     if (rc) return rc;
   }
@@ -509,6 +512,7 @@ int dm_count_cliques(dm_graph* g, int32_t k, const dm_opts* o, uint64_t* count, 
   L.ctr = ws.d_ctr;
   L.queue = ws.d_queue;
   L.qcap = ws.qcap;
+  L.nq = QUEUE_SHARDS;
   L.max_donations = ctx.donations_per_warp;
   DM_CUDA(cudaEventRecord(ws.k0, ctx.stream));
   int grid = 0;
@@ -662,6 +666,7 @@ int dm_count_motifs(dm_graph* g, int32_t k, const dm_dictionary* dict, const dm_
   L.ctr = ws.d_ctr;
   L.queue = ws.d_queue;
   L.qcap = ws.qcap;
+  L.nq = QUEUE_SHARDS;
   L.max_donations = ctx.donations_per_warp;
   L.q2c = ws.d_q2c;
   L.n_classes = dict->n_classes;

@@ -22,6 +22,8 @@ struct alignas(128) DevCounters {
   int pad2[31];
   unsigned long long progress;   // work finished (batched), watched by waiting warps
   unsigned long long pad3[15];
+  int queued;                    // donated tasks in the queue
+  int pad4[31];
   unsigned long long count;      // clique total
   unsigned long long nodes;      // DFS nodes expanded
   unsigned long long tasks;      // tasks executed (roots + donated ranges)
@@ -69,8 +71,9 @@ struct CliqueLaunch {
   const int32_t* roots = nullptr;  // ordered root ranks
   int n_roots = 0;
   DevCounters* ctr = nullptr;
-  void* queue = nullptr;         // donation queue: header + slots (lb.cuh)
-  int qcap = 0;
+  void* queue = nullptr;         // donation queue: nq headers + nq * qcap slots (lb.cuh)
+  int qcap = 0;                  // slots per shard
+  int nq = 1;                    // shards
   int max_donations = 16;        // per task
   int32_t* arena = nullptr;      // list path
   int arena_dcap = 0;
@@ -91,6 +94,7 @@ struct MotifLaunch {
   DevCounters* ctr = nullptr;
   void* queue = nullptr;
   int qcap = 0;
+  int nq = 1;
   int max_donations = 16;
   const int32_t* q2c = nullptr;
   int n_classes = 0;

@@ -11,9 +11,10 @@
 // range in half and enqueues the upper half (a donated DFS prefix). The receiver rebuilds
 // the root's state and runs only the donated items.
 //
-// The queue is a bounded multi-producer multi-consumer ring (per-slot sequence numbers):
-// a consumer only ever takes a slot whose producer has finished writing it, so nothing
-// waits on another warp's store. Termination: `pending` counts roots not yet finished plus
+// The queue is a set of bounded multi-producer multi-consumer rings (per-slot sequence
+// numbers): a consumer only ever takes a slot whose producer has finished writing it, so
+// nothing waits on another warp's store. Donations are demand-limited: a warp donates only
+// while more warps are hungry than tasks are queued. Termination: `pending` counts roots not yet finished plus
 // donated tasks not yet finished (raised before the enqueue). A hungry warp leaves when
 // pending is zero; if nothing changes for timeout_ns it records ERR_TIMEOUT and leaves.
 //
@@ -34,8 +35,11 @@ struct QSlot {
   int end;
 };
 
-// Persistent queue header, followed by `cap` slots. Positions keep running across calls
-// (a call ends with the queue empty); the host re-initialises it after an error.
+// Persistent queue: nq shard headers followed by nq x cap slots (shard s owns slots
+// [s*cap, (s+1)*cap)). Positions keep running across calls (a call ends with the queue
+// empty); the host re-initialises it after an error. A warp pushes to and pops from its home
+// shard first and then the others, so thousands of hungry warps do not all contend on one
+// read position.
 struct QHeader {
   unsigned write_pos;
   unsigned pad0[31];
@@ -45,14 +49,16 @@ struct QHeader {
 
 struct LBArgs {
   DevCounters* ctr;
-  QHeader* qh;
-  QSlot* q;
-  int qcap;
+  QHeader* qh;                // nq shard headers
+  QSlot* q;                   // nq * qcap slots
+  int qcap;                   // slots per shard
   int hungry_trigger;    // donate when at least this many warps are hungry (<= 0: never)
   int max_donations;     // per task
   long long donate_after_ns;  // a task donates only after running this long
   long long timeout_ns;
   int test_stall;             // test hook: wait at exit on a word nothing sets
+  int min_split;              // a task keeps ranges shorter than this
+  int nq;                     // shards
 };
 
 __device__ __forceinline__ long long global_ns() {
@@ -69,15 +75,16 @@ __device__ __forceinline__ unsigned long long vload64(const unsigned long long* 
 
 __device__ __forceinline__ void set_err(DevCounters* c, int code) { atomicCAS(&c->err, 0, code); }
 
-static __device__ __noinline__ bool q_push(const LBArgs& lb, int root, int b, int e) {
-  unsigned pos = vloadu(&lb.qh->write_pos);
-  QSlot* s;
-  for (int tries = 0; tries < 1024; ++tries) {
-    s = lb.q + (pos % (unsigned)lb.qcap);
+static __device__ __forceinline__ bool shard_push(const LBArgs& lb, int sh, int root, int b, int e) {
+  QHeader* h = lb.qh + sh;
+  QSlot* base = lb.q + (size_t)sh * lb.qcap;
+  unsigned pos = vloadu(&h->write_pos);
+  for (int tries = 0; tries < 64; ++tries) {
+    QSlot* s = base + (pos % (unsigned)lb.qcap);
     const unsigned seq = vloadu(&s->seq);
     const int dif = (int)(seq - pos);
     if (dif == 0) {
-      const unsigned prev = atomicCAS(&lb.qh->write_pos, pos, pos + 1);
+      const unsigned prev = atomicCAS(&h->write_pos, pos, pos + 1);
       if (prev == pos) {
         s->root = root;
         s->begin = b;
@@ -88,22 +95,24 @@ static __device__ __noinline__ bool q_push(const LBArgs& lb, int root, int b, in
       }
       pos = prev;
     } else if (dif < 0) {
-      return false;  // full
+      return false;  // this shard is full
     } else {
-      pos = vloadu(&lb.qh->write_pos);
+      pos = vloadu(&h->write_pos);
     }
   }
   return false;
 }
 
-static __device__ __noinline__ bool q_pop(const LBArgs& lb, int& root, int& b, int& e) {
-  unsigned pos = vloadu(&lb.qh->read_pos);
-  for (int tries = 0; tries < 1024; ++tries) {
-    QSlot* s = lb.q + (pos % (unsigned)lb.qcap);
+static __device__ __forceinline__ bool shard_pop(const LBArgs& lb, int sh, int& root, int& b, int& e) {
+  QHeader* h = lb.qh + sh;
+  QSlot* base = lb.q + (size_t)sh * lb.qcap;
+  unsigned pos = vloadu(&h->read_pos);
+  for (int tries = 0; tries < 64; ++tries) {
+    QSlot* s = base + (pos % (unsigned)lb.qcap);
     const unsigned seq = vloadu(&s->seq);
     const int dif = (int)(seq - (pos + 1));
     if (dif == 0) {
-      const unsigned prev = atomicCAS(&lb.qh->read_pos, pos, pos + 1);
+      const unsigned prev = atomicCAS(&h->read_pos, pos, pos + 1);
       if (prev == pos) {
         __threadfence();
         const volatile QSlot* vs = s;
@@ -118,9 +127,28 @@ static __device__ __noinline__ bool q_pop(const LBArgs& lb, int& root, int& b, i
     } else if (dif < 0) {
       return false;  // empty (or a producer is still writing its slot)
     } else {
-      pos = vloadu(&lb.qh->read_pos);
+      pos = vloadu(&h->read_pos);
     }
   }
+  return false;
+}
+
+static __device__ __noinline__ bool q_push(const LBArgs& lb, int home, int root, int b, int e) {
+  for (int i = 0; i < lb.nq; ++i)
+    if (shard_push(lb, (home + i) % lb.nq, root, b, e)) {
+      atomicAdd(&lb.ctr->queued, 1);
+      return true;
+    }
+  return false;
+}
+
+static __device__ __noinline__ bool q_pop(const LBArgs& lb, int home, int& root, int& b, int& e) {
+  if (vload(&lb.ctr->queued) <= 0) return false;
+  for (int i = 0; i < lb.nq; ++i)
+    if (shard_pop(lb, (home + i) % lb.nq, root, b, e)) {
+      atomicSub(&lb.ctr->queued, 1);
+      return true;
+    }
   return false;
 }
 
@@ -153,9 +181,10 @@ static __device__ __noinline__ bool lb_next(const LBArgs& lb, int n_roots, int t
   unsigned backoff = 256;
   unsigned long long polls = 0;
   bool got = false;
+  const int home = (int)((blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) % (unsigned)lb.nq);
   while (true) {
     int root = 0;
-    if (q_pop(lb, root, b, e)) {
+    if (q_pop(lb, home, root, b, e)) {
       first = root;
       count = 1;
       donated = true;
@@ -242,7 +271,8 @@ __device__ __forceinline__ int range_take(unsigned long long* range) {
   return next < end ? next : -1;
 }
 
-// If warps are hungry and the task has run longer than donate_after_ns, splits the upper
+// If more warps are hungry than tasks are queued and the task has run longer than
+// donate_after_ns, splits the upper
 // half of the remaining range off and enqueues it (with cost_tail > 0, item i is taken to
 // cost cost_tail - i and the split halves the remaining cost instead of the item count). Returns true when the queue was full:
 // the split-off items [ob, oe) then belong to the caller, who must run them itself
@@ -253,14 +283,16 @@ __device__ __forceinline__ bool range_maybe_donate(const LBArgs& lb, unsigned lo
                                                    int& oe, int cost_tail = 0) {
   if (lb.hungry_trigger <= 0) return false;
   if (*reinterpret_cast<volatile int*>(donations_left) <= 0) return false;
-  if (vload(&lb.ctr->hungry) < lb.hungry_trigger) return false;
+  // demand: hungry warps not yet served by a queued task
+  const int hungry = vload(&lb.ctr->hungry);
+  if (hungry - vload(&lb.ctr->queued) < lb.hungry_trigger) return false;
   if (global_ns() - task_start < lb.donate_after_ns) return false;
   if (atomicCAS(busy, 0, 1) != 0) return false;
   bool own = false;
   unsigned long long cur = *reinterpret_cast<volatile unsigned long long*>(range);
   while (true) {
     const int next = (int)(unsigned)cur, end = (int)(unsigned)(cur >> 32);
-    if (end - next < 2) break;
+    if (end - next < (lb.min_split > 2 ? lb.min_split : 2)) break;
     int mid = next + (end - next + 1) / 2;
     if (cost_tail > 0) {
       // item i costs about (cost_tail - i): split where the remaining cost halves
@@ -276,12 +308,12 @@ __device__ __forceinline__ bool range_maybe_donate(const LBArgs& lb, unsigned lo
       continue;
     }
     atomicAdd(&lb.ctr->pending, 1);
-    if (q_push(lb, root, mid, end)) {
+    const int home = (int)((blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) % (unsigned)lb.nq);
+    if (q_push(lb, home, root, mid, end)) {
       atomicSub(donations_left, 1);
       atomicAdd(&lb.ctr->donations, 1ull);
     } else {
       atomicSub(&lb.ctr->pending, 1);
-      atomicExch(donations_left, 0);
       ob = mid;
       oe = end;
       own = true;

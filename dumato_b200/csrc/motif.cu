@@ -371,9 +371,9 @@ int motif_launch(const MotifLaunch& L, LaunchCtx& ctx, int* grid) {
   a.roots = L.roots;
   a.n_roots = L.n_roots;
   a.lb = LBArgs{L.ctr, reinterpret_cast<QHeader*>(L.queue),
-                reinterpret_cast<QSlot*>(reinterpret_cast<char*>(L.queue) + sizeof(QHeader)), L.qcap, 0,
+                reinterpret_cast<QSlot*>(reinterpret_cast<char*>(L.queue) + sizeof(QHeader) * L.nq), L.qcap, 0,
                 L.max_donations, (long long)ctx.donate_after_us * 1000ll, (long long)ctx.timeout_ms * 1000000ll,
-                ctx.test_stall};
+                ctx.test_stall, 4, L.nq};
   a.k = L.k;
   a.q2c = L.q2c;
   a.n_classes = L.n_classes;
