@@ -71,7 +71,7 @@ class _Stats(ctypes.Structure):
                 ("mode_used", ctypes.c_int32), ("vwarp_used", ctypes.c_int32), ("grid", ctypes.c_int32),
                 ("block", ctypes.c_int32), ("kernel_launches", ctypes.c_int32), ("reserved", ctypes.c_int32),
                 ("idle_warp_fraction", ctypes.c_double), ("max_task_ms", ctypes.c_double),
-                ("max_task_root", ctypes.c_int32), ("reserved2", ctypes.c_int32)]
+                ("max_task_root", ctypes.c_int32), ("prefix_donations", ctypes.c_int32)]
 
 
 _P = ctypes.c_void_p
@@ -430,12 +430,13 @@ class Stats:
     idle_warp_fraction: float = 0.0
     max_task_ms: float = 0.0
     max_task_root: int = -1
+    prefix_donations: int = 0
 
     @classmethod
     def from_c(cls, s: _Stats) -> "Stats":
         return cls(s.kernel_ms, s.prep_ms, s.tasks, s.donations, s.idle_polls, s.nodes, s.mode_used,
                    s.vwarp_used, s.grid, s.block, s.kernel_launches, s.idle_warp_fraction, s.max_task_ms,
-                   s.max_task_root)
+                   s.max_task_root, s.prefix_donations)
 
 
 def clique_work_model(g: Graph, k: int) -> tuple[int, int]:
@@ -448,6 +449,7 @@ def clique_work_model(g: Graph, k: int) -> tuple[int, int]:
 
 
 TEST_STALL_AT_EXIT = 1
+TEST_EAGER_DONATION = 2
 
 
 def plan_roots(g: Graph, k: int, clique: bool = True, opts: Optional[Options] = None) -> tuple[np.ndarray, np.ndarray]:

@@ -442,7 +442,8 @@ __global__ void __launch_bounds__(256) clique_kernel(CliqueArgs a) {
   while (true) {
     int first = 0, count = 0, b = 0, e = -1, ok = 0;
     bool donated = false;
-    if (lane == 0) ok = lb_next(a.lb, a.n_roots, total_warps, first, count, b, e, donated) ? 1 : 0;
+    int level = 0, path[QPATH];
+    if (lane == 0) ok = lb_next(a.lb, a.n_roots, total_warps, first, count, b, e, donated, level, path) ? 1 : 0;
     ok = __shfl_sync(FULL_MASK, ok, 0);
     if (!ok) break;
     first = __shfl_sync(FULL_MASK, first, 0);

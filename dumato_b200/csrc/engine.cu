@@ -57,7 +57,7 @@ __global__ void queue_init_kernel(QHeader* h, QSlot* q, int nq, int cap) {
   }
   if (i < nq * cap) {
     q[i].seq = (unsigned)(i % cap);
-    q[i].root = q[i].begin = q[i].end = 0;
+    q[i].root = q[i].begin = q[i].end = q[i].level = 0;
   }
 }
 
@@ -133,6 +133,7 @@ static int select_device(const dm_opts* o, LaunchCtx& ctx) {
     ctx.threshold = o->threshold > 0 ? o->threshold : 0;
     ctx.donations_per_warp = o->donations_per_warp > 0 ? o->donations_per_warp : 16;
     ctx.test_stall = (o->test_flags & DM_TEST_STALL_AT_EXIT) ? 1 : 0;
+    if (o->test_flags & DM_TEST_EAGER_DONATION) ctx.donate_after_us = 0;
   }
   return DM_OK;
 }
@@ -558,6 +559,7 @@ int dm_count_cliques(dm_graph* g, int32_t k, const dm_opts* o, uint64_t* count, 
     st->idle_warp_fraction = warp_ns > 0 ? std::min(1.0, (double)h.hungry_ns / warp_ns) : 0.0;
     st->max_task_ms = (double)h.max_task_ns * 1e-6;
     st->max_task_root = h.max_task_root;
+    st->prefix_donations = (int32_t)std::min<unsigned long long>(h.prefix_donations, INT32_MAX);
   }
   return DM_OK;
 }
@@ -713,6 +715,7 @@ int dm_count_motifs(dm_graph* g, int32_t k, const dm_dictionary* dict, const dm_
     st->idle_warp_fraction = warp_ns > 0 ? std::min(1.0, (double)h.hungry_ns / warp_ns) : 0.0;
     st->max_task_ms = (double)h.max_task_ns * 1e-6;
     st->max_task_root = h.max_task_root;
+    st->prefix_donations = (int32_t)std::min<unsigned long long>(h.prefix_donations, INT32_MAX);
   }
   return DM_OK;
 }

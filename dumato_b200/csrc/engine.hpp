@@ -31,6 +31,7 @@ struct alignas(128) DevCounters {
   unsigned long long idle_polls; // polls of the donation queue by hungry warps
   unsigned long long hungry_ns;  // time warps spent waiting for work, summed over warps
   unsigned long long max_task_ns;  // longest single task
+  unsigned long long prefix_donations;  // donated DFS prefixes (a level >= 1 extension set)
   int max_task_root;             // its root (best effort under races)
   int test_gate;                 // never written by the library (failure-path tests)
   int err;                       // first error code raised by a kernel (0 = none)

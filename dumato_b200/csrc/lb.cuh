@@ -28,11 +28,19 @@
 
 namespace dmb {
 
+// A queued task. level 0: items [begin, end) of root's first level. level L >= 1 (motifs):
+// positions [begin, end) of the extension set at DFS level L, reached from the root along
+// path[0] (the second vertex's index in E_0) and path[1..L-1] (the chosen index at each
+// level below L) - a donated DFS prefix.
+constexpr int QPATH = 7;
 struct QSlot {
   unsigned seq;
   int root;
   int begin;
   int end;
+  int level;
+  int path[QPATH];
+  int pad[4];
 };
 
 // Persistent queue: nq shard headers followed by nq x cap slots (shard s owns slots
@@ -75,7 +83,8 @@ __device__ __forceinline__ unsigned long long vload64(const unsigned long long* 
 
 __device__ __forceinline__ void set_err(DevCounters* c, int code) { atomicCAS(&c->err, 0, code); }
 
-static __device__ __forceinline__ bool shard_push(const LBArgs& lb, int sh, int root, int b, int e) {
+static __device__ __forceinline__ bool shard_push(const LBArgs& lb, int sh, int root, int b, int e, int level,
+                                                  const int* path) {
   QHeader* h = lb.qh + sh;
   QSlot* base = lb.q + (size_t)sh * lb.qcap;
   unsigned pos = vloadu(&h->write_pos);
@@ -89,6 +98,8 @@ static __device__ __forceinline__ bool shard_push(const LBArgs& lb, int sh, int 
         s->root = root;
         s->begin = b;
         s->end = e;
+        s->level = level;
+        for (int i = 0; i < level && i < QPATH; ++i) s->path[i] = path[i];
         __threadfence();
         atomicExch(&s->seq, pos + 1);
         return true;
@@ -103,7 +114,8 @@ static __device__ __forceinline__ bool shard_push(const LBArgs& lb, int sh, int 
   return false;
 }
 
-static __device__ __forceinline__ bool shard_pop(const LBArgs& lb, int sh, int& root, int& b, int& e) {
+static __device__ __forceinline__ bool shard_pop(const LBArgs& lb, int sh, int& root, int& b, int& e, int& level,
+                                                 int* path) {
   QHeader* h = lb.qh + sh;
   QSlot* base = lb.q + (size_t)sh * lb.qcap;
   unsigned pos = vloadu(&h->read_pos);
@@ -119,6 +131,8 @@ static __device__ __forceinline__ bool shard_pop(const LBArgs& lb, int sh, int& 
         root = vs->root;
         b = vs->begin;
         e = vs->end;
+        level = vs->level;
+        for (int i = 0; i < level && i < QPATH; ++i) path[i] = vs->path[i];
         __threadfence();
         atomicExch(&s->seq, pos + (unsigned)lb.qcap);
         return true;
@@ -133,19 +147,21 @@ static __device__ __forceinline__ bool shard_pop(const LBArgs& lb, int sh, int& 
   return false;
 }
 
-static __device__ __noinline__ bool q_push(const LBArgs& lb, int home, int root, int b, int e) {
+static __device__ __noinline__ bool q_push(const LBArgs& lb, int home, int root, int b, int e, int level,
+                                           const int* path) {
   for (int i = 0; i < lb.nq; ++i)
-    if (shard_push(lb, (home + i) % lb.nq, root, b, e)) {
+    if (shard_push(lb, (home + i) % lb.nq, root, b, e, level, path)) {
       atomicAdd(&lb.ctr->queued, 1);
       return true;
     }
   return false;
 }
 
-static __device__ __noinline__ bool q_pop(const LBArgs& lb, int home, int& root, int& b, int& e) {
+static __device__ __noinline__ bool q_pop(const LBArgs& lb, int home, int& root, int& b, int& e, int& level,
+                                          int* path) {
   if (vload(&lb.ctr->queued) <= 0) return false;
   for (int i = 0; i < lb.nq; ++i)
-    if (shard_pop(lb, (home + i) % lb.nq, root, b, e)) {
+    if (shard_pop(lb, (home + i) % lb.nq, root, b, e, level, path)) {
       atomicSub(&lb.ctr->queued, 1);
       return true;
     }
@@ -155,8 +171,8 @@ static __device__ __noinline__ bool q_pop(const LBArgs& lb, int home, int& root,
 // Lane-0 only. Claims a chunk of roots [first, first+count) from the cursor, or failing
 // that a donated task (count = 1, range [b, e)). Returns false when all work is done or an
 // error was raised.
-static __device__ __noinline__ bool lb_next(const LBArgs& lb, int n_roots, int total_warps, int& first, int& count, int& b, int& e,
-                        bool& donated) {
+static __device__ __noinline__ bool lb_next(const LBArgs& lb, int n_roots, int total_warps, int& first, int& count,
+                                            int& b, int& e, bool& donated, int& level, int* path) {
   DevCounters* c = lb.ctr;
   int cur = vload(&c->cursor);
   if (cur < n_roots) {
@@ -169,6 +185,7 @@ static __device__ __noinline__ bool lb_next(const LBArgs& lb, int n_roots, int t
       count = min(chunk, n_roots - r);
       b = 0;
       e = -1;
+      level = 0;
       donated = false;
       return true;
     }
@@ -184,7 +201,7 @@ static __device__ __noinline__ bool lb_next(const LBArgs& lb, int n_roots, int t
   const int home = (int)((blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) % (unsigned)lb.nq);
   while (true) {
     int root = 0;
-    if (q_pop(lb, home, root, b, e)) {
+    if (q_pop(lb, home, root, b, e, level, path)) {
       first = root;
       count = 1;
       donated = true;
@@ -271,6 +288,17 @@ __device__ __forceinline__ int range_take(unsigned long long* range) {
   return next < end ? next : -1;
 }
 
+// Split point of items [next, end) (at least two): the midpoint, or with cost_tail > 0 (item
+// i costs about cost_tail - i) the point where the remaining cost halves.
+__device__ __forceinline__ int split_mid(int next, int end, int cost_tail) {
+  if (cost_tail <= 0) return next + (end - next + 1) / 2;
+  const double a = (double)(cost_tail - next) + 0.5;
+  const double total = 0.5 * (double)(end - next) * (double)((cost_tail - next) + (cost_tail - end + 1));
+  const double disc = a * a - total;
+  const int x = (int)(a - sqrt(disc > 0 ? disc : 0.0) + 0.5);
+  return next + max(1, min(end - next - 1, x));
+}
+
 // If more warps are hungry than tasks are queued and the task has run longer than
 // donate_after_ns, splits the upper
 // half of the remaining range off and enqueues it (with cost_tail > 0, item i is taken to
@@ -293,15 +321,7 @@ __device__ __forceinline__ bool range_maybe_donate(const LBArgs& lb, unsigned lo
   while (true) {
     const int next = (int)(unsigned)cur, end = (int)(unsigned)(cur >> 32);
     if (end - next < (lb.min_split > 2 ? lb.min_split : 2)) break;
-    int mid = next + (end - next + 1) / 2;
-    if (cost_tail > 0) {
-      // item i costs about (cost_tail - i): split where the remaining cost halves
-      const double a = (double)(cost_tail - next) + 0.5;
-      const double total = 0.5 * (double)(end - next) * (double)((cost_tail - next) + (cost_tail - end + 1));
-      const double disc = a * a - total;
-      const int x = (int)(a - sqrt(disc > 0 ? disc : 0.0) + 0.5);
-      mid = next + max(1, min(end - next - 1, x));
-    }
+    const int mid = split_mid(next, end, cost_tail);
     const unsigned long long prev = atomicCAS(range, cur, pack_range(next, mid));
     if (prev != cur) {
       cur = prev;
@@ -309,7 +329,7 @@ __device__ __forceinline__ bool range_maybe_donate(const LBArgs& lb, unsigned lo
     }
     atomicAdd(&lb.ctr->pending, 1);
     const int home = (int)((blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) % (unsigned)lb.nq);
-    if (q_push(lb, home, root, mid, end)) {
+    if (q_push(lb, home, root, mid, end, 0, nullptr)) {
       atomicSub(donations_left, 1);
       atomicAdd(&lb.ctr->donations, 1ull);
     } else {
@@ -322,6 +342,28 @@ __device__ __forceinline__ bool range_maybe_donate(const LBArgs& lb, unsigned lo
   }
   atomicExch(busy, 0);
   return own;
+}
+
+// Demand test shared by the donation paths (lane 0): hungry warps outnumber queued tasks by
+// the trigger and the task has run long enough.
+__device__ __forceinline__ bool lb_wants_donation(const LBArgs& lb, const int* donations_left, long long task_start) {
+  if (lb.hungry_trigger <= 0) return false;
+  if (*reinterpret_cast<const volatile int*>(donations_left) <= 0) return false;
+  if (vload(&lb.ctr->hungry) - vload(&lb.ctr->queued) < lb.hungry_trigger) return false;
+  return global_ns() - task_start >= lb.donate_after_ns;
+}
+
+// Enqueues a deep task (lane 0). Returns false when every shard is full.
+__device__ __forceinline__ bool lb_donate_deep(const LBArgs& lb, int root, int level, const int* path, int b, int e) {
+  atomicAdd(&lb.ctr->pending, 1);
+  const int home = (int)((blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) % (unsigned)lb.nq);
+  if (q_push(lb, home, root, b, e, level, path)) {
+    atomicAdd(&lb.ctr->donations, 1ull);
+    if (level > 0) atomicAdd(&lb.ctr->prefix_donations, 1ull);
+    return true;
+  }
+  atomicSub(&lb.ctr->pending, 1);
+  return false;
 }
 
 }  // namespace dmb

@@ -24,7 +24,10 @@
 // is cheaper), then each non-empty mask bucket adds to one class counter.
 //
 // Work is warp-cooperative: a task is (v0, range of second vertices); lane 0 takes items,
-// the warp runs the subtree, and idle warps get donated item ranges (lb.cuh).
+// the warp runs the subtree, and idle warps get donated work (lb.cuh): either a range of
+// second vertices or, when one second vertex roots most of the work (a hub), a DFS prefix -
+// the path to some level's extension set and a range of its members, which the receiver
+// rebuilds by replaying the path (each level's set is a deterministic function of the path).
 #include <algorithm>
 #include <climits>
 #include <string>
@@ -57,16 +60,42 @@ struct MotifArgs {
 __host__ __device__ constexpr int quick_off(int p) { return (p - 2) * (p + 1) / 2; }
 
 // Per-warp shared state.
-struct MotifWarp {
+struct alignas(16) MotifWarp {
   unsigned long long range;
   int donations_left;
   int busy;
   int n[MOTIF_KMAX];           // extension-set sizes per level
   int pos[MOTIF_KMAX];         // next member to expand per level
+  int lim[MOTIF_KMAX];         // members [pos, lim) of a level are still this warp's to expand
   int runn[MOTIF_KMAX];        // run sizes per level
   unsigned quick[MOTIF_KMAX];  // quick code of the prefix ending at level t
   unsigned mh[64];             // leaf-mask histogram
+  unsigned sh[32];             // masks of E_{k-3}[pos..n): the members still above the current vertex
 };
+
+// First index in [lo, hi) of an id-sorted (vertex, mask) list whose vertex is >= x.
+__device__ __forceinline__ int lower_bound2(const int2* a, int lo, int hi, int32_t x) {
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (a[mid].x < x) lo = mid + 1; else hi = mid;
+  }
+  return lo;
+}
+
+__device__ __forceinline__ int ilog2p1(int x) { return 32 - __clz(x | 1); }
+
+// Adds the masks of list[lo, hi) to the warp's 32-entry histogram h (warp-aggregated).
+__device__ __forceinline__ void mask_hist(const int2* list, int lo, int hi, unsigned* h) {
+  for (int i0 = lo; i0 < hi; i0 += 32) {
+    const int i = i0 + lane_id();
+    const bool v = i < hi;
+    const int m = v ? list[i].y : -1;
+    const unsigned act = __ballot_sync(FULL_MASK, v);
+    const unsigned same = __match_any_sync(FULL_MASK, m);
+    if (v && (same & act & ((1u << lane_id()) - 1u)) == 0) atomicAdd(&h[m], (unsigned)__popc(same & act));
+  }
+  __syncwarp();
+}
 
 // Membership of x in the disjoint sorted runs 0..t (run 0 is the CSR suffix of v0).
 __device__ __forceinline__ bool in_runs(int32_t x, const int32_t* run0, int n0, const int2* const* runs,
@@ -82,6 +111,44 @@ __device__ __forceinline__ bool in_runs(int32_t x, const int32_t* run0, int n0, 
     if (lo < runn[i] && r[lo].x == x) return true;
   }
   return false;
+}
+
+// Lane 0, between two expansions of a task whose lowest own level is `floor` (1 for an item
+// task; L for a donated DFS prefix of level L) and whose deepest materialised level is t:
+// when warps are hungry, hands the upper half of the shallowest level that still has two
+// unexpanded members to the queue. Level 0 is the task's second-vertex range (cost-aware
+// split); a level s >= 1 goes out as (root, s, path to E_s, position range), the path being
+// the second vertex's index `it` and the index picked at each level 1..s-1.
+__device__ __forceinline__ void motif_try_donate(const LBArgs& lb, MotifWarp* sw, int v0, int floor, int t, int it,
+                                                 int n0, long long t_start) {
+  if (!lb_wants_donation(lb, &sw->donations_left, t_start)) return;
+  if (floor == 1) {
+    const unsigned long long cur = sw->range;
+    const int next = (int)(unsigned)cur, end = (int)(unsigned)(cur >> 32);
+    if (end - next >= 2) {
+      const int mid = split_mid(next, end, n0);
+      if (lb_donate_deep(lb, v0, 0, nullptr, mid, end)) {
+        sw->range = pack_range(next, mid);
+        sw->donations_left -= 1;
+      }
+      return;
+    }
+  }
+  for (int s = floor; s <= t; ++s) {
+    const int ps = sw->pos[s], lim = sw->lim[s];
+    if (lim - ps >= 2) {
+      // E_s is sorted by id: member i inherits the n - i - 1 members above it
+      const int mid = split_mid(ps, lim, sw->n[s]);
+      int path[QPATH];
+      path[0] = it;
+      for (int j = 1; j < s && j < QPATH; ++j) path[j] = sw->pos[j] - 1;
+      if (lb_donate_deep(lb, v0, s, path, mid, lim)) {
+        sw->lim[s] = mid;
+        sw->donations_left -= 1;
+      }
+      return;
+    }
+  }
 }
 
 // Flushes the warp's leaf-mask histogram into the block's class counters.
@@ -136,16 +203,28 @@ __global__ void __launch_bounds__(32 * MOTIF_WARPS) motif_kernel(MotifArgs a) {
   }
   unsigned long long ntasks = 0, nodes = 0;
   while (true) {
-    int first = 0, count = 0, b = 0, e = -1, ok = 0;
+    int first = 0, count = 0, b = 0, e = -1, ok = 0, level = 0;
+    int path[QPATH];
+    for (int j = 0; j < QPATH; ++j) path[j] = 0;
     bool donated = false;
-    if (lane == 0) ok = lb_next(a.lb, a.n_roots, total_warps, first, count, b, e, donated) ? 1 : 0;
+    if (lane == 0) ok = lb_next(a.lb, a.n_roots, total_warps, first, count, b, e, donated, level, path) ? 1 : 0;
     ok = __shfl_sync(FULL_MASK, ok, 0);
     if (!ok) break;
     first = __shfl_sync(FULL_MASK, first, 0);
     count = __shfl_sync(FULL_MASK, count, 0);
     b = __shfl_sync(FULL_MASK, b, 0);
     e = __shfl_sync(FULL_MASK, e, 0);
+    level = __shfl_sync(FULL_MASK, level, 0);
+    for (int j = 0; j < K - 3 && j < QPATH; ++j) path[j] = __shfl_sync(FULL_MASK, path[j], 0);
     donated = __shfl_sync(FULL_MASK, donated ? 1 : 0, 0) != 0;
+    // a donated DFS prefix names a level that this k has
+    if (level < 0 || level > K - 3) {
+      if (lane == 0) {
+        set_err(a.lb.ctr, ERR_BAD_TASK);
+        lb_done(a.lb, count);
+      }
+      break;
+    }
     for (int ti = 0; ti < count; ++ti) {
       const int v0 = donated ? first : __ldg(a.roots + first + ti);
       int bb = b, ee = e;
@@ -159,8 +238,15 @@ __global__ void __launch_bounds__(32 * MOTIF_WARPS) motif_kernel(MotifArgs a) {
       const int s0 = lower_bound(row0, 0, deg0, v0 + 1);
       const int32_t* E0 = row0 + s0;
       const int n0 = deg0 - s0;
+      // level >= 1: replay the path down to E_level, then expand positions [b, e) there
+      const int floor = level > 0 ? level : 1;
       int lo, hi;
-      task_range(bb, ee, n0, lo, hi);
+      if (level > 0) {
+        lo = 0;
+        hi = 0;
+      } else {
+        task_range(bb, ee, n0, lo, hi);
+      }
       if (lane == 0) {
         sw->range = pack_range(lo, hi);
         sw->donations_left = a.lb.max_donations;
@@ -168,53 +254,101 @@ __global__ void __launch_bounds__(32 * MOTIF_WARPS) motif_kernel(MotifArgs a) {
         sw->quick[0] = 0;
       }
       __syncwarp();
+      bool replay_item = level > 0;
       while (true) {
         int it = 0;
-        if (lane == 0) {
-          it = range_take(&sw->range);
-          int ob = 0, oe = 0;
-          if (it >= 0 &&
-              range_maybe_donate(a.lb, &sw->range, v0, &sw->donations_left, t_start, &sw->busy, ob, oe, n0)) {
-            // lane 0 is the only taker, so the split can be undone
-            const unsigned long long cur = *reinterpret_cast<volatile unsigned long long*>(&sw->range);
-            sw->range = (cur & 0xffffffffull) | ((unsigned long long)(unsigned)oe << 32);
+        if (replay_item) {
+          it = path[0];
+          replay_item = false;
+          if (it < 0 || it >= n0) {
+            if (lane == 0) set_err(a.lb.ctr, ERR_BAD_TASK);
+            break;
           }
+        } else if (level > 0) {
+          break;
+        } else {
+          if (lane == 0) {
+            it = range_take(&sw->range);
+            int ob = 0, oe = 0;
+            if (it >= 0 &&
+                range_maybe_donate(a.lb, &sw->range, v0, &sw->donations_left, t_start, &sw->busy, ob, oe, n0)) {
+              // lane 0 is the only taker, so the split can be undone
+              const unsigned long long cur = *reinterpret_cast<volatile unsigned long long*>(&sw->range);
+              sw->range = (cur & 0xffffffffull) | ((unsigned long long)(unsigned)oe << 32);
+            }
+          }
+          it = __shfl_sync(FULL_MASK, it, 0);
+          if (it < 0) break;
         }
-        it = __shfl_sync(FULL_MASK, it, 0);
-        if (it < 0) break;
         // prefix (v0, w1); the members of E_0 after w1 are the inherited part
         int t = 0;
         int w = __ldg(E0 + it);
         int wmask = 1;
         int src_lo = it + 1;  // level 0: inherited members are E0[it+1 ..]
+        bool bad = false;
         // depth-first over levels; level t's current vertex is w with mask wmask
         while (true) {
           // here the prefix is v_0..v_t plus w = v_{t+1}
-          ++nodes;
-          if (lane == 0 && (nodes & 255) == 0) atomicAdd(&a.lb.ctr->progress, 256ull);
           const int p = t + 1;  // position of w
+          if (p > level) {
+            // nodes at or above a donated prefix's level belong to the donor
+            ++nodes;
+            if (lane == 0 && (nodes & 255) == 0) atomicAdd(&a.lb.ctr->progress, 256ull);
+          }
           unsigned quick_p = (t == 0) ? 0u : sw->quick[t];
           if (p >= 2) quick_p += ((unsigned)wmask & ((1u << p) - 1u)) << quick_off(p);
           const int32_t* Nw = a.g.adj + __ldg(a.g.row + w);
           const int dw = __ldg(a.g.deg + w);
-          // inherited members: e in E_t with e > w
+          // inherited members: e in E_t with e > w. E_t is sorted by vertex id and w is its
+          // member at position pos[t] - 1 (E_0: index it), so they are the suffix from there.
           const int2* Et = (t == 0) ? nullptr : ext_c[t];
           const int nE = (t == 0) ? n0 : sw->n[t];
-          const int startE = (t == 0) ? src_lo : 0;
+          const int startE = (t == 0) ? src_lo : sw->pos[t];
           if (p == K - 2) {
             // leaves: histogram the masks of E_{p} without writing it
             const int leaf_off = quick_off(K - 1);
-            for (int i = startE + lane; i < nE; i += 32) {
-              int ev, em;
+            const int n_inh = nE - startE;
+            const int gt = lower_bound(Nw, 0, dw, w + 1);
+            const int dgt = dw - gt;
+            // probe each inherited member in N(w), or take the suffix's mask counts and
+            // move the members found in N(w) above w (whichever side is cheaper)
+            if ((long long)dgt * ilog2p1(n_inh) + (1 << (K - 2)) < (long long)n_inh * ilog2p1(dw)) {
               if (t == 0) {
-                ev = __ldg(E0 + i);
-                em = 1;
-              } else {
-                const int2 x = Et[i];
-                ev = x.x;
-                em = x.y;
+                if (lane == 0 && n_inh) atomicAdd(&sw->mh[1], (unsigned)n_inh);
+              } else if (lane < (1 << (K - 2))) {
+                const unsigned c = sw->sh[lane];
+                if (c) atomicAdd(&sw->mh[lane], c);
               }
-              if (ev > w) {
+              __syncwarp();
+              for (int i = gt + lane; i < dw; i += 32) {
+                const int32_t x = Nw[i];
+                int em = -1;
+                if (t == 0) {
+                  const int j = lower_bound(E0, startE, n0, x);
+                  if (j < n0 && __ldg(E0 + j) == x) em = 1;
+                } else {
+                  const int j = lower_bound2(Et, startE, nE, x);
+                  if (j < nE) {
+                    const int2 y = Et[j];
+                    if (y.x == x) em = y.y;
+                  }
+                }
+                if (em >= 0) {
+                  atomicSub(&sw->mh[em], 1u);
+                  atomicAdd(&sw->mh[em | (1 << p)], 1u);
+                }
+              }
+            } else {
+              for (int i = startE + lane; i < nE; i += 32) {
+                int ev, em;
+                if (t == 0) {
+                  ev = __ldg(E0 + i);
+                  em = 1;
+                } else {
+                  const int2 x = Et[i];
+                  ev = x.x;
+                  em = x.y;
+                }
                 const int m = em | (contains(Nw, dw, ev) ? (1 << p) : 0);
                 atomicAdd(&sw->mh[m], 1u);
               }
@@ -236,7 +370,7 @@ __global__ void __launch_bounds__(32 * MOTIF_WARPS) motif_kernel(MotifArgs a) {
             } else {
               // iterate N(w) above v0, probe the runs
               for (int i = sw0 + lane; i < dw; i += 32)
-                inter += in_runs(__ldg(Nw + i), E0, n0, runs_c, sw->runn, t) ? 1u : 0u;
+                inter += in_runs(Nw[i], E0, n0, runs_c, sw->runn, t) ? 1u : 0u;
             }
             for (int o = 16; o > 0; o >>= 1) inter += __shfl_xor_sync(FULL_MASK, inter, o);
             if (lane == 0) {
@@ -246,30 +380,11 @@ __global__ void __launch_bounds__(32 * MOTIF_WARPS) motif_kernel(MotifArgs a) {
             __syncwarp();
             flush_masks(sw, a, quick_p, leaf_off, bhist, task_cnt);
           } else {
-            // materialise E_{p} = inherited + excl(w); excl(w) also becomes run p
+            // materialise E_{p} = inherited + excl(w), merged by vertex id; excl(w) is also
+            // run p. Both parts are sorted and disjoint, so each member's place is its index
+            // in its own part plus the number of smaller members of the other part.
             int2* Ep = ext[p];
             int2* Rp = runs[p];
-            int m = 0;
-            for (int i0 = startE; i0 < nE; i0 += 32) {
-              const int i = i0 + lane;
-              int ev = 0, em = 0;
-              bool keep = false;
-              if (i < nE) {
-                if (t == 0) {
-                  ev = __ldg(E0 + i);
-                  em = 1;
-                } else {
-                  const int2 x = Et[i];
-                  ev = x.x;
-                  em = x.y;
-                }
-                keep = ev > w;
-                if (keep && contains(Nw, dw, ev)) em |= 1 << p;
-              }
-              const unsigned bal = __ballot_sync(FULL_MASK, keep);
-              if (keep) Ep[m + __popc(bal & ((1u << lane) - 1u))] = make_int2(ev, em);
-              m += __popc(bal);
-            }
             const int sw0 = lower_bound(Nw, 0, dw, v0 + 1);
             int rn = 0;
             for (int i0 = sw0; i0 < dw; i0 += 32) {
@@ -277,36 +392,88 @@ __global__ void __launch_bounds__(32 * MOTIF_WARPS) motif_kernel(MotifArgs a) {
               int32_t x = 0;
               bool nw = false;
               if (i < dw) {
-                x = __ldg(Nw + i);
+                x = Nw[i];
                 nw = !in_runs(x, E0, n0, runs_c, sw->runn, t);
               }
               const unsigned bal = __ballot_sync(FULL_MASK, nw);
-              if (nw) {
-                const int q = __popc(bal & ((1u << lane) - 1u));
-                Rp[rn + q] = make_int2(x, 0);
-                Ep[m + q] = make_int2(x, 1 << p);
-              }
+              if (nw) Rp[rn + __popc(bal & ((1u << lane) - 1u))] = make_int2(x, 0);
               rn += __popc(bal);
-              m += __popc(bal);
             }
             __syncwarp();
+            for (int i = startE + lane; i < nE; i += 32) {
+              int ev, em;
+              if (t == 0) {
+                ev = __ldg(E0 + i);
+                em = 1;
+              } else {
+                const int2 x = Et[i];
+                ev = x.x;
+                em = x.y;
+              }
+              if (contains(Nw, dw, ev)) em |= 1 << p;
+              Ep[(i - startE) + lower_bound2(Rp, 0, rn, ev)] = make_int2(ev, em);
+            }
+            for (int j = lane; j < rn; j += 32) {
+              const int32_t x = Rp[j].x;
+              const int c = (t == 0) ? lower_bound(E0, 0, n0, x) : lower_bound2(Et, 0, nE, x);
+              Ep[j + max(0, c - startE)] = make_int2(x, 1 << p);
+            }
+            const int m = (nE - startE) + rn;
+            __syncwarp();
+            if (p < level) {
+              // replaying a donated prefix: the path fixes the member expanded at level p
+              const int idx = (p < QPATH) ? path[p] : -1;
+              if (idx < 0 || idx >= m) {
+                if (lane == 0) set_err(a.lb.ctr, ERR_BAD_TASK);
+                bad = true;
+                break;
+              }
+              const int2 x = Ep[idx];
+              if (lane == 0) {
+                sw->n[p] = m;
+                sw->pos[p] = idx + 1;
+                sw->lim[p] = idx + 1;
+                sw->runn[p] = rn;
+                sw->quick[p] = quick_p;
+              }
+              __syncwarp();
+              t = p;
+              w = x.x;
+              wmask = x.y;
+              continue;
+            }
+            const int first_pos = p == level ? min(b, m) : 0;
             if (lane == 0) {
               sw->n[p] = m;
-              sw->pos[p] = 0;
+              sw->pos[p] = first_pos;
+              sw->lim[p] = p == level ? min(e, m) : m;
               sw->runn[p] = rn;
               sw->quick[p] = quick_p;
+            }
+            if (p == K - 3) {
+              sw->sh[lane] = 0;
+              __syncwarp();
+              mask_hist(Ep, first_pos, m, sw->sh);
             }
             __syncwarp();
             t = p;  // descend; pick the first member below
           }
+          // give work away when warps are hungry (checked every 16 expansions)
+          if ((nodes & 15) == 0 && K >= 4) {
+            if (lane == 0) motif_try_donate(a.lb, sw, v0, floor, t, it, n0, t_start);
+            __syncwarp();
+          }
           // next vertex: advance the deepest level that still has members
           bool found = false;
-          while (t >= 1) {
+          while (t >= floor) {
             const int ps = sw->pos[t];
-            if (ps < sw->n[t]) {
+            if (ps < sw->lim[t]) {
               const int2 x = ext_c[t][ps];
               __syncwarp();
-              if (lane == 0) sw->pos[t] = ps + 1;
+              if (lane == 0) {
+                sw->pos[t] = ps + 1;
+                if (t == K - 3) sw->sh[x.y] -= 1u;
+              }
               __syncwarp();
               w = x.x;
               wmask = x.y;
@@ -317,6 +484,7 @@ __global__ void __launch_bounds__(32 * MOTIF_WARPS) motif_kernel(MotifArgs a) {
           }
           if (!found) break;
         }
+        if (bad) break;
       }
       if (a.per_root) {
         const unsigned long long tsum = warp_sum_u64(task_cnt);

@@ -23,8 +23,8 @@
 
 namespace dmb {
 
-// Donation-queue slots held by the fixed scratch (16 bytes each).
-constexpr int NOALLOC_QUEUE_SLOTS = 16384;
+// Donation-queue slots held by the fixed scratch (64 bytes each).
+constexpr int NOALLOC_QUEUE_SLOTS = 4096;
 // Largest out-degree the fixed scratch supports: roots up to this size run on the bitmap
 // path, which needs no per-warp arena.
 constexpr int NOALLOC_MAX_OUT_DEGREE = 256;
@@ -46,7 +46,7 @@ __global__ void noalloc_queue_init(QHeader* h, QSlot* q, int cap) {
   }
   if (i < cap) {
     q[i].seq = (unsigned)i;
-    q[i].root = q[i].begin = q[i].end = 0;
+    q[i].root = q[i].begin = q[i].end = q[i].level = 0;
   }
 }
 

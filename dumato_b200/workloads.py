@@ -22,3 +22,34 @@ def make(name: str, seed: int = 1):
     p = dict(CONFIGS[name])
     kind = p.pop("kind")
     return Graph.generate(kind, p.pop("n"), p.pop("m"), seed=seed, **p)
+
+
+def main(argv=None) -> int:
+    """Runs one query on a named workload `reps` times and prints the last run's count and
+    kernel time (the command line the kernel profiles are taken with)."""
+    import argparse
+
+    from . import Dictionary, count_cliques, count_motifs
+
+    ap = argparse.ArgumentParser(prog="python -m dumato_b200.workloads")
+    ap.add_argument("query", choices=("clique", "motif"))
+    ap.add_argument("workload", choices=sorted(CONFIGS))
+    ap.add_argument("k", type=int)
+    ap.add_argument("--reps", type=int, default=2)
+    ap.add_argument("--seed", type=int, default=1)
+    args = ap.parse_args(argv)
+    g = make(args.workload, args.seed)
+    d = Dictionary.generate(args.k) if args.query == "motif" else None
+    for _ in range(max(1, args.reps)):
+        if d is None:
+            total, st = count_cliques(g, args.k)
+        else:
+            hist, st = count_motifs(g, args.k, d)
+            total = int(hist.sum())
+    print(f"{args.query} {args.workload} k={args.k}: {total} in {st.kernel_ms:.3f} ms "
+          f"(tasks {st.tasks}, donations {st.donations}, prefix donations {st.prefix_donations})")
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

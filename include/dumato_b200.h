@@ -114,6 +114,8 @@ typedef struct dm_opts {
    wait expires and the call returns DM_ETIMEOUT (exercises the timeout path without a
    fault or a hang; use a short timeout_ms). */
 #define DM_TEST_STALL_AT_EXIT 1
+/* donations need no minimum task age, so small inputs exercise the donation paths */
+#define DM_TEST_EAGER_DONATION 2
 
 typedef struct dm_stats {
   double kernel_ms;            /* device time of the counting kernels (CUDA events) */
@@ -131,7 +133,7 @@ typedef struct dm_stats {
   double idle_warp_fraction;   /* time warps waited for work / (warps x kernel time) */
   double max_task_ms;          /* longest single task (root or donated range) */
   int32_t max_task_root;       /* its root (cliques: rank space; motifs: vertex id) */
-  int32_t reserved2;
+  int32_t prefix_donations;    /* of the donations, DFS prefixes below the first level (motifs) */
 } dm_stats;
 
 /* ---- version / errors ---- */

@@ -140,3 +140,30 @@ def test_matches_reference_binaries(dm, gpu, tmp_path):
             for cls, cnt in mot["classes"].items():
                 want[int(cls)] = cnt
             assert np.array_equal(got, want), (name, k)
+
+
+def _hub_graph(hub_deg, seed):
+    """Vertex 0 (the lowest id, so a root) is adjacent to hub 1 and a few others; the hub has
+    `hub_deg` neighbours, so the item (root 0, second vertex 1) holds most of the work."""
+    rng = np.random.default_rng(seed)
+    n = 600
+    src = [0] * 11 + [1] * hub_deg
+    dst = [1] + list(rng.choice(np.arange(2, n), 10, replace=False)) + list(rng.choice(np.arange(2, n), hub_deg, replace=False))
+    s, t = rng.integers(2, n, 1500), rng.integers(2, n, 1500)
+    return np.concatenate([np.array(src), s]), np.concatenate([np.array(dst), t])
+
+
+@pytest.mark.parametrize("k,hub_deg", [(4, 250), (5, 120), (6, 60), (7, 36)])
+def test_hub_item_split_by_prefix_donation(dm, orc, gpu, k, hub_deg):
+    """Donated DFS prefixes (path replay on the receiving warp) give the oracle's counts."""
+    src, dst = _hub_graph(hub_deg, seed=k)
+    g = dm.Graph.from_edges(src, dst)
+    og = orc.OracleGraph.from_pairs(*g.edges())
+    d, q2c = _dict(dm, k)
+    want = orc.motifs(og, k, q2c, d.n_classes)
+    plain, _ = dm.count_motifs(g, k, d)
+    assert np.array_equal(plain, want)
+    for _ in range(2):
+        eager, st = dm.count_motifs(g, k, d, dm.Options(test_flags=dm.TEST_EAGER_DONATION))
+        assert np.array_equal(eager, want)
+        assert st.prefix_donations > 0 and st.donations >= st.prefix_donations
