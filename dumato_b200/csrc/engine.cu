@@ -645,7 +645,8 @@ int dm_count_motifs(dm_graph* g, int32_t k, const dm_dictionary* dict, const dm_
   DM_CUDA(cudaMemsetAsync(ws.d_hist, 0, sizeof(unsigned long long) * dict->n_classes, ctx.stream));
   // arena: extension levels and runs per warp
   const int maxdeg = std::max(g->max_degree, 1);
-  const size_t per_warp = motif_arena_stride(k, maxdeg) * sizeof(int2);
+  const int vwarp = (ctx.vwarp == 8 || ctx.vwarp == 16) ? ctx.vwarp : 32;
+  const size_t per_warp = motif_arena_stride(k, maxdeg, vwarp) * sizeof(int2);
   const size_t budget = (size_t)8 << 30;
   ctx.arena_warps = (int)std::min<size_t>((size_t)ctx.num_sms * 64, std::max<size_t>(8, budget / per_warp));
   if ((rc = ensure_ws_bytes(&ws.d_scratch, &ws.scratch_cap, per_warp * ctx.arena_warps))) return rc;
@@ -676,6 +677,7 @@ int dm_count_motifs(dm_graph* g, int32_t k, const dm_dictionary* dict, const dm_
   L.arena = ws.d_scratch;
   L.maxdeg = maxdeg;
   L.per_root = want_log ? ws.d_per_root : nullptr;
+  L.vwarp = vwarp;
   DM_CUDA(cudaEventRecord(ws.k0, ctx.stream));
   int grid = 0;
   if (n_roots > 0) {
@@ -707,7 +709,7 @@ int dm_count_motifs(dm_graph* g, int32_t k, const dm_dictionary* dict, const dm_
     st->idle_polls = h.idle_polls;
     st->nodes = h.nodes;
     st->mode_used = DM_MODE_LIST;
-    st->vwarp_used = 32;
+    st->vwarp_used = vwarp;
     st->grid = grid;
     st->block = 256;
     st->kernel_launches = ctx.launches;

@@ -104,9 +104,10 @@ struct MotifLaunch {
   int maxdeg = 0;
   unsigned long long* per_root = nullptr;
   const int32_t* parts = nullptr;
+  int vwarp = 32;                // virtual-warp width: 8, 16 or 32
 };
 int motif_launch(const MotifLaunch& L, LaunchCtx& ctx, int* grid);
-size_t motif_arena_stride(int k, int maxdeg);  // int2 slots per warp
+size_t motif_arena_stride(int k, int maxdeg, int vwarp);  // int2 slots per warp
 
 const char* cuda_err_str(cudaError_t e);
 

@@ -302,13 +302,14 @@ __device__ __forceinline__ int split_mid(int next, int end, int cost_tail) {
 // If more warps are hungry than tasks are queued and the task has run longer than
 // donate_after_ns, splits the upper
 // half of the remaining range off and enqueues it (with cost_tail > 0, item i is taken to
-// cost cost_tail - i and the split halves the remaining cost instead of the item count). Returns true when the queue was full:
+// cost cost_tail - i and the split halves the remaining cost instead of the item count; a
+// range is split only with at least min_items (default lb.min_split) left). Returns true when the queue was full:
 // the split-off items [ob, oe) then belong to the caller, who must run them itself
 // (lanes that find the range empty have already moved the cursor past `mid`, so the split
 // cannot simply be undone). `busy` serialises donations of one warp.
 __device__ __forceinline__ bool range_maybe_donate(const LBArgs& lb, unsigned long long* range, int root,
                                                    int* donations_left, long long task_start, int* busy, int& ob,
-                                                   int& oe, int cost_tail = 0) {
+                                                   int& oe, int cost_tail = 0, int min_items = 0) {
   if (lb.hungry_trigger <= 0) return false;
   if (*reinterpret_cast<volatile int*>(donations_left) <= 0) return false;
   // demand: hungry warps not yet served by a queued task
@@ -320,7 +321,8 @@ __device__ __forceinline__ bool range_maybe_donate(const LBArgs& lb, unsigned lo
   unsigned long long cur = *reinterpret_cast<volatile unsigned long long*>(range);
   while (true) {
     const int next = (int)(unsigned)cur, end = (int)(unsigned)(cur >> 32);
-    if (end - next < (lb.min_split > 2 ? lb.min_split : 2)) break;
+    const int need = min_items > 0 ? min_items : lb.min_split;
+    if (end - next < (need > 2 ? need : 2)) break;
     const int mid = split_mid(next, end, cost_tail);
     const unsigned long long prev = atomicCAS(range, cur, pack_range(next, mid));
     if (prev != cur) {

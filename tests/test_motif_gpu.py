@@ -167,3 +167,30 @@ def test_hub_item_split_by_prefix_donation(dm, orc, gpu, k, hub_deg):
         eager, st = dm.count_motifs(g, k, d, dm.Options(test_flags=dm.TEST_EAGER_DONATION))
         assert np.array_equal(eager, want)
         assert st.prefix_donations > 0 and st.donations >= st.prefix_donations
+
+
+@pytest.mark.parametrize("vwarp", [8, 16])
+@pytest.mark.parametrize("k", [3, 4, 5, 6])
+def test_virtual_warps_vs_oracle(dm, orc, gpu, vwarp, k):
+    """Groups of 8 or 16 lanes sharing a task's second vertices give the oracle's counts."""
+    from dumato_b200 import workloads
+
+    g = workloads.make("er2k", 2)
+    og = orc.OracleGraph.from_pairs(*g.edges())
+    d, q2c = _dict(dm, k)
+    want = orc.motifs(og, k, q2c, d.n_classes)
+    got, st = dm.count_motifs(g, k, d, dm.Options(vwarp=vwarp))
+    assert st.vwarp_used == vwarp
+    assert np.array_equal(got, want)
+
+
+@pytest.mark.parametrize("vwarp", [8, 16])
+def test_virtual_warps_with_prefix_donation(dm, orc, gpu, vwarp):
+    src, dst = _hub_graph(120, seed=5)
+    g = dm.Graph.from_edges(src, dst)
+    og = orc.OracleGraph.from_pairs(*g.edges())
+    d, q2c = _dict(dm, 5)
+    want = orc.motifs(og, 5, q2c, d.n_classes)
+    got, st = dm.count_motifs(g, 5, d, dm.Options(vwarp=vwarp, test_flags=dm.TEST_EAGER_DONATION))
+    assert np.array_equal(got, want)
+    assert st.prefix_donations > 0
