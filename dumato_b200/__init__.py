@@ -34,6 +34,8 @@ STATUS_NAMES = {
 
 GEN_ER, GEN_CHUNG_LU, GEN_RMAT = 0, 1, 2
 MODE_AUTO, MODE_LIST, MODE_BITMAP = 0, 1, 2
+QUERY_CLIQUE, QUERY_MOTIF = 0, 1
+AUTOTUNE_MODEL, AUTOTUNE_MEASURE = 0, 1
 SCHED_PLAIN, SCHED_LEARNED, SCHED_ID = 0, 1, 2
 
 
@@ -74,6 +76,18 @@ class _Stats(ctypes.Structure):
                 ("max_task_root", ctypes.c_int32), ("prefix_donations", ctypes.c_int32)]
 
 
+class _Query(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int32), ("k", ctypes.c_int32), ("graph", ctypes.c_void_p),
+                ("dict", ctypes.c_void_p), ("vwarp", ctypes.c_int32), ("threshold", ctypes.c_int32),
+                ("mode", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+
+
+class _QueryTuning(ctypes.Structure):
+    _fields_ = [("vwarp", ctypes.c_int32), ("threshold", ctypes.c_int32), ("mode", ctypes.c_int32),
+                ("n_results", ctypes.c_int32), ("result_offset", ctypes.c_int64), ("tune_ms", ctypes.c_double),
+                ("est_cost", ctypes.c_double)]
+
+
 _P = ctypes.c_void_p
 _SIGNATURES = {
     "dm_abi_version": (ctypes.c_int, []),
@@ -112,6 +126,12 @@ _SIGNATURES = {
                                                 ctypes.c_int32, ctypes.c_uint64, _P]),
     "dm_count_cliques": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.POINTER(_Opts), _P, ctypes.POINTER(_Stats)]),
     "dm_count_motifs": (ctypes.c_int, [_P, ctypes.c_int32, _P, ctypes.POINTER(_Opts), _P, ctypes.POINTER(_Stats)]),
+    "dm_batch_create": (ctypes.c_int, [ctypes.POINTER(_Query), ctypes.c_int32, ctypes.POINTER(_Opts), ctypes.c_int32,
+                                       ctypes.POINTER(_P)]),
+    "dm_batch_num_results": (ctypes.c_int64, [_P]),
+    "dm_batch_tuning": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.POINTER(_QueryTuning)]),
+    "dm_batch_run": (ctypes.c_int, [_P, _P, ctypes.c_int64, ctypes.POINTER(_Stats)]),
+    "dm_batch_free": (None, [_P]),
 }
 
 _lib: Optional[ctypes.CDLL] = None
@@ -484,3 +504,83 @@ def count_motifs(g: Graph, k: int, dictionary: Optional[Dictionary] = None,
     st = _Stats()
     _check(lib().dm_count_motifs(g.handle, int(k), d.handle, ctypes.byref(o), _ptr(out), ctypes.byref(st)))
     return out, Stats.from_c(st)
+
+
+@dataclass
+class Query:
+    """One (graph, query) pair of a batch: k-cliques (kind QUERY_CLIQUE, k in 2..6) or motif
+    class counts (QUERY_MOTIF, k in 3..5). vwarp / threshold / mode left at 0 / -1 / MODE_AUTO
+    are chosen by the autotuner."""
+    kind: int
+    k: int
+    graph: Graph
+    dictionary: Optional[Dictionary] = None
+    vwarp: int = 0
+    threshold: int = -1
+    mode: int = MODE_AUTO
+
+
+@dataclass
+class QueryTuning:
+    vwarp: int
+    threshold: int
+    mode: int
+    n_results: int
+    result_offset: int
+    tune_ms: float
+    est_cost: float
+
+
+class Batch:
+    """Many (graph, query) pairs counted by one persistent, CUDA-graph-captured launch.
+
+    Built once (union graph upload, autotuning, capture); run() replays the launch and returns
+    one result per query: an int (k-cliques) or a uint64 array of class counts (motifs)."""
+
+    def __init__(self, queries: Sequence[Query], autotune: int = AUTOTUNE_MODEL, opts: Optional[Options] = None):
+        self._queries = list(queries)
+        arr = (_Query * max(1, len(self._queries)))()
+        for i, q in enumerate(self._queries):
+            if q.kind == QUERY_MOTIF and q.dictionary is None:
+                raise ValueError(f"query {i}: a motif query needs its k-vertex dictionary")
+            arr[i] = _Query(kind=q.kind, k=q.k, graph=q.graph.handle,
+                            dict=q.dictionary.handle if q.dictionary is not None else None,
+                            vwarp=q.vwarp, threshold=q.threshold, mode=q.mode)
+        o = (opts or Options()).to_c()
+        h = _P()
+        _check(lib().dm_batch_create(arr, len(self._queries), ctypes.byref(o), int(autotune), ctypes.byref(h)))
+        self._h = h
+        self.n_results = int(lib().dm_batch_num_results(h))
+
+    def tuning(self, i: int) -> QueryTuning:
+        t = _QueryTuning()
+        _check(lib().dm_batch_tuning(self._h, int(i), ctypes.byref(t)))
+        return QueryTuning(t.vwarp, t.threshold, t.mode, t.n_results, t.result_offset, t.tune_ms, t.est_cost)
+
+    def run_raw(self, out: Optional[np.ndarray] = None) -> tuple[np.ndarray, Stats]:
+        """All result words (uint64[n_results]) of one replay, and its stats."""
+        if out is None:
+            out = np.zeros(max(1, self.n_results), np.uint64)
+        st = _Stats()
+        _check(lib().dm_batch_run(self._h, _ptr(out), out.size, ctypes.byref(st)))
+        return out, Stats.from_c(st)
+
+    def run(self) -> tuple[list, Stats]:
+        raw, st = self.run_raw()
+        res = []
+        for i, q in enumerate(self._queries):
+            t = self.tuning(i)
+            part = raw[t.result_offset:t.result_offset + t.n_results]
+            res.append(int(part[0]) if q.kind == QUERY_CLIQUE else part.copy())
+        return res, st
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) is not None:
+            lib().dm_batch_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

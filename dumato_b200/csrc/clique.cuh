@@ -1,0 +1,462 @@
+// k-clique enumeration for sm_100a: the per-task device code (bitmap and list paths).
+//
+// Semantics: the number of k-vertex cliques, each counted once, as the reference's clique
+// driver computes (src/main/clique_PA.cu:9-32 with extend_clique, DuMatoGPU.cu:1194-1220:
+// C_l = {u in N(v_l) : u > v_l} cap C_{l-1}, the leaf level adding |C_{k-2}| through
+// aggregate_counter, DuMatoGPU.cu:1769-1771). The reference breaks symmetry by vertex id on
+// the undirected graph; here the graph is oriented by (degree, id) rank, which counts the
+// same cliques with out-degrees bounded by O(sqrt(m)).
+//
+// One persistent launch runs every root. A root's work is split into items that lanes (or
+// warps) pull dynamically, and idle warps receive donated item ranges (lb.cuh):
+//   bitmap path (out-degree d <= 64*NWMAX, NWMAX <= 4): the warp builds the local
+//       adjacency bitmap of the root's out-neighbourhood L in shared memory (bit j of row i
+//       set iff L[j] in N+(L[i])). Items are the local edges (c1, c2); a lane takes an item
+//       and counts the (k-3)-cliques of row[c1] & row[c2] by its own DFS over 64-bit words:
+//       extend = AND of two rows, compact = nothing (bit order is candidate order),
+//       aggregate = popc at the last level.
+//   list path (larger d, or DM_MODE_LIST): the reference's list structure. Items are the
+//       first-level candidates c1; the warp extends sorted candidate lists level by level in
+//       a per-warp global arena by binary-search intersection and ballot compaction
+//       (DuMatoGPU.cu:317-328 write), counting the leaf level without writing it.
+#pragma once
+
+#include <climits>
+
+#include "engine.hpp"
+#include "gpm.cuh"
+#include "lb.cuh"
+
+namespace dmb {
+
+template <int NW>
+struct Bits {
+  uint64_t w[NW];
+};
+
+template <int NW>
+__device__ __forceinline__ int popc(const Bits<NW>& s) {
+  int c = 0;
+#pragma unroll
+  for (int i = 0; i < NW; ++i) c += __popcll(s.w[i]);
+  return c;
+}
+
+// Number of (D+1)-cliques inside the local vertex set S (rows: NW u64 words per row).
+template <int D, int NW>
+__device__ __forceinline__ unsigned long long count_rec(const Bits<NW>& S, const uint64_t* __restrict__ rows) {
+  if constexpr (D == 0) {
+    return (unsigned long long)popc(S);
+  } else {
+    unsigned long long sum = 0;
+#pragma unroll
+    for (int wi = 0; wi < NW; ++wi) {
+      uint64_t bits = S.w[wi];
+      while (bits) {
+        const int b = __ffsll((long long)bits) - 1;
+        bits &= bits - 1;
+        const uint64_t* rc = rows + (wi * 64 + b) * NW;
+        Bits<NW> T;
+#pragma unroll
+        for (int j = 0; j < NW; ++j) T.w[j] = (j < wi ? 0ull : (j == wi ? bits : S.w[j])) & rc[j];
+        if constexpr (D == 1) {
+          sum += (unsigned long long)popc(T);
+        } else {
+          if (popc(T) >= D) sum += count_rec<D - 1, NW>(T, rows);
+        }
+      }
+    }
+    return sum;
+  }
+}
+
+// Position of the j-th (0-based) set bit of an NW-word row.
+template <int NW>
+__device__ __forceinline__ int select_bit(const uint64_t* row, int j) {
+#pragma unroll
+  for (int w = 0; w < NW; ++w) {
+    const uint64_t x = row[w];
+    const int pc = __popcll(x);
+    if (j < pc) {
+      const unsigned lo = (unsigned)x;
+      const int pl = __popc(lo);
+      if (j < pl) return w * 64 + (int)__fns(lo, 0, j + 1);
+      return w * 64 + 32 + (int)__fns((unsigned)(x >> 32), 0, j - pl + 1);
+    }
+    j -= pc;
+  }
+  return -1;
+}
+
+// Shared memory of one warp for a launch whose bitmap roots need up to M words per row:
+// rows | L | prefix of out-degrees | prefix of row popcounts | item range | list stack.
+struct WarpLayout {
+  int rows, L, P, E, range, don, busy, hn, heavy, ptr, n, pos, total;
+};
+
+__host__ __device__ constexpr WarpLayout warp_layout(int M) {
+  WarpLayout w{};
+  w.rows = 0;
+  w.L = 512 * M * M;
+  w.P = w.L + 4 * 64 * M;
+  w.E = w.P + 4 * (64 * M + 1);
+  w.range = (w.E + 4 * (64 * M + 1) + 7) / 8 * 8;
+  w.don = w.range + 8;
+  w.busy = w.don + 4;
+  w.hn = w.busy + 4;
+  w.heavy = w.hn + 4;  // 32 deferred heavy items
+  w.ptr = (w.heavy + 4 * 32 + 7) / 8 * 8;
+  w.n = w.ptr + 8 * 16;
+  w.pos = w.n + 4 * 16;
+  w.total = (w.pos + 4 * 16 + 15) / 16 * 16;
+  return w;
+}
+
+struct CliqueArgs {
+  GraphView g;
+  const int32_t* roots;
+  int n_roots;
+  LBArgs lb;
+  const int32_t* parts;         // optional per-root-entry part word (p | P << 16), else null
+  int32_t* arena;               // list path: K * arena_dcap ints per warp
+  int arena_dcap;
+  int list_threshold;           // roots with d > list_threshold take the list path
+  unsigned long long* per_root; // optional: k-cliques found under each root (subtree logger)
+};
+
+// Loads L = N+(root) into shared memory and the exclusive prefix sum of the out-degrees
+// of its members (sP[0..d]). Returns the total.
+static __device__ __forceinline__ int load_root_list(const GraphView& g, int root, int d, int32_t* sL, int32_t* sP) {
+  const int lane = lane_id();
+  const int32_t* L = g.adj + __ldg(g.row + root);
+  int carry = 0;
+  for (int i0 = 0; i0 < d; i0 += 32) {
+    const int i = i0 + lane;
+    int u = 0, du = 0;
+    if (i < d) {
+      u = __ldg(L + i);
+      du = __ldg(g.deg + u);
+      sL[i] = u;
+    }
+    int s = du;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      int y = __shfl_up_sync(FULL_MASK, s, o);
+      if (lane >= o) s += y;
+    }
+    if (i < d) sP[i] = carry + s - du;
+    carry += __shfl_sync(FULL_MASK, s, 31);
+  }
+  if (lane == 0) sP[d] = carry;
+  __syncwarp();
+  return carry;
+}
+
+// Local adjacency bitmap of L (rows zeroed by the caller): the (member, out-neighbour)
+// pairs are flattened so the warp stays busy when rows are short; membership in L is a
+// binary search in shared memory.
+static __device__ __forceinline__ void build_local_rows(const GraphView& g, const int32_t* sL, const int32_t* sP, int d,
+                                                 int total, uint32_t* rows, int row_words) {
+  const int lane = lane_id();
+  const int32_t maxL = sL[d - 1];
+  for (int f = lane; f < total; f += 32) {
+    const int i = lower_bound(sP, 0, d + 1, f + 1) - 1;  // largest i with sP[i] <= f
+    const int32_t x = __ldg(g.adj + __ldg(g.row + sL[i]) + (f - sP[i]));
+    if (x <= maxL) {
+      const int j = lower_bound(sL, i + 1, d, x);
+      if (j < d && sL[j] == x) atomicOr(rows + i * row_words + (j >> 5), 1u << (j & 31));
+    }
+  }
+}
+
+constexpr int HEAVY_BITS = 24;  // an item whose candidate set has this many members is
+                                // run by the whole warp instead of one lane (k >= 6)
+constexpr int HEAVY_SLOTS = 32;
+
+// Counts the cliques of item `it` (a local edge c1 < c2, or a row c1 when k == 3) on one
+// lane. For k >= 6 an item with a large candidate set is deferred to the warp instead
+// (returns without counting) when a heavy slot is free.
+template <int K, int NW>
+__device__ __forceinline__ unsigned long long bitmap_item(int it, const uint64_t* rows, const int32_t* sE, int d,
+                                                          int* hn, int* heavy) {
+  if constexpr (K == 3) {
+    Bits<NW> S;
+#pragma unroll
+    for (int w = 0; w < NW; ++w) S.w[w] = rows[it * NW + w];
+    return (unsigned long long)popc(S);
+  } else {
+    const int c1 = lower_bound(sE, 0, d + 1, it + 1) - 1;
+    const int c2 = select_bit<NW>(rows + c1 * NW, it - sE[c1]);
+    Bits<NW> S;
+#pragma unroll
+    for (int w = 0; w < NW; ++w) S.w[w] = rows[c1 * NW + w] & rows[c2 * NW + w];
+    if constexpr (K == 4) {
+      return (unsigned long long)popc(S);
+    } else {
+      const int p = popc(S);
+      if (p < K - 3) return 0;
+      if constexpr (K >= 6) {
+        if (p >= HEAVY_BITS && hn) {
+          const int slot = atomicAdd(hn, 1);
+          if (slot < HEAVY_SLOTS) {
+            heavy[slot] = it;
+            return 0;
+          }
+        }
+      }
+      return count_rec<(K >= 5 ? K - 4 : 0), NW>(S, rows);
+    }
+  }
+}
+
+// Warp-cooperative run of one heavy item: the third local vertex c3 is spread over the
+// lanes (the j-th member of the candidate set goes to lane j mod 32).
+template <int K, int NW>
+__device__ __forceinline__ unsigned long long heavy_item(int it, const uint64_t* rows, const int32_t* sE, int d) {
+  const int lane = lane_id();
+  const int c1 = lower_bound(sE, 0, d + 1, it + 1) - 1;
+  const int c2 = select_bit<NW>(rows + c1 * NW, it - sE[c1]);
+  Bits<NW> S;
+#pragma unroll
+  for (int w = 0; w < NW; ++w) S.w[w] = rows[c1 * NW + w] & rows[c2 * NW + w];
+  unsigned long long sum = 0;
+  int j = 0;
+#pragma unroll
+  for (int wi = 0; wi < NW; ++wi) {
+    uint64_t bits = S.w[wi];
+    while (bits) {
+      const int b = __ffsll((long long)bits) - 1;
+      bits &= bits - 1;
+      if ((j++ & 31) != lane) continue;
+      const uint64_t* rc = rows + (wi * 64 + b) * NW;
+      Bits<NW> T;
+#pragma unroll
+      for (int w = 0; w < NW; ++w) T.w[w] = (w < wi ? 0ull : (w == wi ? bits : S.w[w])) & rc[w];
+      if (popc(T) >= K - 4) sum += count_rec<(K >= 6 ? K - 5 : 0), NW>(T, rows);
+    }
+  }
+  return sum;
+}
+
+// Bitmap path for one task. Returns the k-cliques counted by this lane.
+template <int K, int NW, int M>
+__device__ unsigned long long bitmap_task(const CliqueArgs& a, unsigned char* wsm, int root, int d, int b, int e) {
+  constexpr WarpLayout LY = warp_layout(M);
+  constexpr int RW = 2 * NW;
+  const int lane = lane_id();
+  uint32_t* rows32 = reinterpret_cast<uint32_t*>(wsm + LY.rows);
+  int32_t* sL = reinterpret_cast<int32_t*>(wsm + LY.L);
+  int32_t* sP = reinterpret_cast<int32_t*>(wsm + LY.P);
+  int32_t* sE = reinterpret_cast<int32_t*>(wsm + LY.E);
+  unsigned long long* range = reinterpret_cast<unsigned long long*>(wsm + LY.range);
+  int* donations_left = reinterpret_cast<int*>(wsm + LY.don);
+  int* busy = reinterpret_cast<int*>(wsm + LY.busy);
+  int* hn = reinterpret_cast<int*>(wsm + LY.hn);
+  int* heavy = reinterpret_cast<int*>(wsm + LY.heavy);
+  const long long t_start = global_ns();
+  for (int i = lane; i < d * RW; i += 32) rows32[i] = 0;
+  const int total = load_root_list(a.g, root, d, sL, sP);
+  build_local_rows(a.g, sL, sP, d, total, rows32, RW);
+  __syncwarp();
+  const uint64_t* rows = reinterpret_cast<const uint64_t*>(rows32);
+  int n_items;
+  if constexpr (K >= 4) {
+    // exclusive prefix of row popcounts: the items are the local edges
+    int carry = 0;
+    for (int i0 = 0; i0 < d; i0 += 32) {
+      const int i = i0 + lane;
+      int pc = 0;
+      if (i < d) {
+#pragma unroll
+        for (int w = 0; w < NW; ++w) pc += __popcll(rows[i * NW + w]);
+      }
+      int s = pc;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        int y = __shfl_up_sync(FULL_MASK, s, o);
+        if (lane >= o) s += y;
+      }
+      if (i < d) sE[i] = carry + s - pc;
+      carry += __shfl_sync(FULL_MASK, s, 31);
+    }
+    if (lane == 0) sE[d] = carry;
+    n_items = carry;
+  } else {
+    n_items = d;
+  }
+  int lo, hi;
+  task_range(b, e, n_items, lo, hi);
+  if (lane == 0) {
+    *range = pack_range(lo, hi);
+    *donations_left = a.lb.max_donations;
+    *busy = 0;
+    *hn = 0;
+  }
+  __syncwarp();
+  unsigned long long cnt = 0;
+  unsigned done = 0;
+  while (true) {
+    const int it = range_take(range);
+    if (it < 0) break;
+    cnt += bitmap_item<K, NW>(it, rows, sE, d, hn, heavy);
+    if ((++done & 15) == 0) {
+      int ob = 0, oe = 0;
+      if (range_maybe_donate(a.lb, range, root, donations_left, t_start, busy, ob, oe)) {
+        for (int j = ob; j < oe; ++j) cnt += bitmap_item<K, NW>(j, rows, sE, d, nullptr, nullptr);
+      }
+      if ((done & 255) == 0) atomicAdd(&a.lb.ctr->progress, 256ull);
+    }
+  }
+  __syncwarp();
+  if constexpr (K >= 6) {
+    const int nh = min(*hn, HEAVY_SLOTS);
+    for (int h = 0; h < nh; ++h) {
+      cnt += heavy_item<K, NW>(heavy[h], rows, sE, d);
+      if (lane == 0) atomicAdd(&a.lb.ctr->progress, 1ull);
+    }
+    __syncwarp();
+  }
+  return cnt;
+}
+
+// List path for one task (warp-cooperative). Returns this lane's share of the count.
+template <int K, int M>
+__device__ unsigned long long list_task(const CliqueArgs& a, unsigned char* wsm, int root, int d, int b, int e,
+                                        int32_t* my_arena) {
+  constexpr WarpLayout LY = warp_layout(M);
+  const int lane = lane_id();
+  unsigned long long* range = reinterpret_cast<unsigned long long*>(wsm + LY.range);
+  int* donations_left = reinterpret_cast<int*>(wsm + LY.don);
+  int* busy = reinterpret_cast<int*>(wsm + LY.busy);
+  const long long t_start = global_ns();
+  const int32_t** sPtr = reinterpret_cast<const int32_t**>(wsm + LY.ptr);
+  int* sN = reinterpret_cast<int*>(wsm + LY.n);
+  int* sPos = reinterpret_cast<int*>(wsm + LY.pos);
+  const int32_t* L = a.g.adj + __ldg(a.g.row + root);
+  int lo, hi;
+  task_range(b, e, d, lo, hi);
+  if (lane == 0) {
+    *range = pack_range(lo, hi);
+    *donations_left = a.lb.max_donations;
+    *busy = 0;
+  }
+  __syncwarp();
+  unsigned long long cnt = 0;
+  while (true) {
+    int it = 0;
+    if (lane == 0) {
+      it = range_take(range);
+      int ob = 0, oe = 0;
+      if (it >= 0 && range_maybe_donate(a.lb, range, root, donations_left, t_start, busy, ob, oe)) {
+        // lane 0 is the only taker here, so the split can be undone
+        const unsigned long long cur = *reinterpret_cast<volatile unsigned long long*>(range);
+        *range = (cur & 0xffffffffull) | ((unsigned long long)(unsigned)oe << 32);
+      }
+    }
+    it = __shfl_sync(FULL_MASK, it, 0);
+    if (it < 0) break;
+    const int c = __ldg(L + it);
+    const int32_t* A = L + it + 1;
+    const int na = d - it - 1;
+    if (na < K - 2) continue;
+    const int32_t* B = a.g.adj + __ldg(a.g.row + c);
+    const int nb = __ldg(a.g.deg + c);
+    if constexpr (K == 3) {
+      unsigned s = 0;
+      for (int i = lane; i < na; i += 32) s += contains(B, nb, __ldg(A + i)) ? 1u : 0u;
+      cnt += s;
+    } else {
+      // C1 = A cap N+(c), written to level 1 of the arena
+      int32_t* out1 = my_arena + a.arena_dcap;
+      int m = 0;
+      for (int i0 = 0; i0 < na; i0 += 32) {
+        const int i = i0 + lane;
+        const int32_t x = i < na ? __ldg(A + i) : 0;
+        m += compact(out1, m, x, i < na && contains(B, nb, x));
+      }
+      __syncwarp();
+      if (lane == 0) {
+        sPtr[1] = out1;
+        sN[1] = m;
+        sPos[1] = 0;
+      }
+      __syncwarp();
+      int lvl = 1;
+      while (lvl >= 1) {
+        const int pos = sPos[lvl];
+        const int rem = sN[lvl] - pos;
+        if (rem - 1 < K - 2 - lvl) {
+          --lvl;
+          continue;
+        }
+        const int32_t* P = sPtr[lvl];
+        const int v = P[pos];
+        __syncwarp();
+        if (lane == 0) {
+          sPos[lvl] = pos + 1;
+          if ((pos & 63) == 63) atomicAdd(&a.lb.ctr->progress, 64ull);
+        }
+        const int32_t* A2 = P + pos + 1;
+        const int na2 = rem - 1;
+        const int32_t* B2 = a.g.adj + __ldg(a.g.row + v);
+        const int nb2 = __ldg(a.g.deg + v);
+        if (lvl + 1 == K - 2) {
+          unsigned s = 0;
+          for (int i = lane; i < na2; i += 32) s += contains(B2, nb2, A2[i]) ? 1u : 0u;
+          cnt += s;
+        } else {
+          int32_t* out = my_arena + (size_t)(lvl + 1) * a.arena_dcap;
+          int m2 = 0;
+          for (int i0 = 0; i0 < na2; i0 += 32) {
+            const int i = i0 + lane;
+            const int32_t x = i < na2 ? A2[i] : 0;
+            m2 += compact(out, m2, x, i < na2 && contains(B2, nb2, x));
+          }
+          __syncwarp();
+          ++lvl;
+          if (lane == 0) {
+            sPtr[lvl] = out;
+            sN[lvl] = m2;
+            sPos[lvl] = 0;
+          }
+        }
+        __syncwarp();
+      }
+    }
+  }
+  __syncwarp();
+  return cnt;
+}
+
+// One root task: items [b, e) of root (task_range encoding), on the bitmap path when the
+// out-degree d is at most a.list_threshold (local bitmaps of ceil(d/64) <= M words per row),
+// else on the list path (needs `arena` with room for K lists of a.arena_dcap ids). Returns
+// this lane's share of the k-cliques found.
+template <int K, int M>
+__device__ __forceinline__ unsigned long long clique_task(const CliqueArgs& a, unsigned char* wsm, int root, int b,
+                                                          int e, int32_t* arena) {
+  const int lane = lane_id();
+  const int d = __ldg(a.g.deg + root);
+  unsigned long long task_cnt = 0;
+  if (e >= 0 && b >= e) {
+    // empty donation: nothing to do
+  } else if (K == 2) {
+    if (lane == 0) task_cnt = (unsigned long long)d;
+  } else if (d > a.list_threshold) {
+    if (K > 3 && (!arena || d > a.arena_dcap)) {
+      if (lane == 0) set_err(a.lb.ctr, ERR_ARENA_OVERFLOW);
+    } else {
+      task_cnt = list_task<K, M>(a, wsm, root, d, b, e, arena);
+    }
+  } else {
+    const int nw = (d + 63) >> 6;
+    if (nw <= 1) task_cnt = bitmap_task<K, 1, M>(a, wsm, root, d, b, e);
+    else if (M >= 2 && nw == 2) task_cnt = bitmap_task<K, (M >= 2 ? 2 : 1), M>(a, wsm, root, d, b, e);
+    else if (M >= 3 && nw == 3) task_cnt = bitmap_task<K, (M >= 3 ? 3 : 1), M>(a, wsm, root, d, b, e);
+    else if (M >= 4 && nw == 4) task_cnt = bitmap_task<K, (M >= 4 ? 4 : 1), M>(a, wsm, root, d, b, e);
+    else if (lane == 0) set_err(a.lb.ctr, ERR_BAD_TASK);
+  }
+  return task_cnt;
+}
+
+}  // namespace dmb

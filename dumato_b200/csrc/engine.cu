@@ -45,8 +45,6 @@ struct Workspace {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, k0 = nullptr, k1 = nullptr;
 };
 
-constexpr int QUEUE_SHARDS = 64;
-constexpr int QUEUE_SHARD_SLOTS = 2048;
 
 // Empty state: every shard's positions at 0, slot j of a shard carrying sequence j.
 __global__ void queue_init_kernel(QHeader* h, QSlot* q, int nq, int cap) {
@@ -59,6 +57,14 @@ __global__ void queue_init_kernel(QHeader* h, QSlot* q, int nq, int cap) {
     q[i].seq = (unsigned)(i % cap);
     q[i].root = q[i].begin = q[i].end = q[i].level = 0;
   }
+}
+
+int queue_init_launch(void* queue, int nq, int cap, cudaStream_t st) {
+  QHeader* h = reinterpret_cast<QHeader*>(queue);
+  QSlot* q = reinterpret_cast<QSlot*>(reinterpret_cast<char*>(queue) + sizeof(QHeader) * nq);
+  queue_init_kernel<<<(nq * cap + 255) / 256, 256, 0, st>>>(h, q, nq, cap);
+  DM_CUDA(cudaGetLastError());
+  return DM_OK;
 }
 
 static int init_queue(Workspace& ws, cudaStream_t st) {
@@ -96,7 +102,7 @@ static std::mutex g_dev_mu;
 static std::map<int, cudaStream_t> g_streams;
 static std::map<int, int> g_sms;
 
-static int select_device(const dm_opts* o, LaunchCtx& ctx) {
+int select_device(const dm_opts* o, LaunchCtx& ctx) {
   int count = 0;
   cudaError_t e = cudaGetDeviceCount(&count);
   if (e != cudaSuccess || count == 0) {
@@ -265,7 +271,7 @@ static int upload_parts(Workspace& ws, const std::vector<int32_t>& parts, cudaSt
   return DM_OK;
 }
 
-static int check_opts(const dm_opts* o) {
+int check_opts(const dm_opts* o) {
   if (!o) return DM_OK;
   if (o->struct_size != 0 && o->struct_size != (int32_t)sizeof(dm_opts))
     return fail(DM_EINVAL, "dm_opts.struct_size does not match this library");

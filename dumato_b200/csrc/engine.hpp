@@ -111,6 +111,13 @@ size_t motif_arena_stride(int k, int maxdeg, int vwarp);  // int2 slots per warp
 
 const char* cuda_err_str(cudaError_t e);
 
+// Host helpers shared by the entry points (engine.cu).
+int select_device(const dm_opts* o, LaunchCtx& ctx);   // device, stream and options -> ctx
+int check_opts(const dm_opts* o);
+int queue_init_launch(void* queue, int nq, int cap, cudaStream_t st);  // empty donation queue
+constexpr int QUEUE_SHARDS = 64;        // donation-queue shards of a workspace
+constexpr int QUEUE_SHARD_SLOTS = 2048; // slots per shard
+
 }  // namespace dmb
 
 #define DM_CUDA(call)                                                              \

@@ -174,6 +174,52 @@ DM_API int dm_count_cliques(dm_graph* g, int32_t k, const dm_opts* opts, uint64_
 DM_API int dm_count_motifs(dm_graph* g, int32_t k, const dm_dictionary* dict, const dm_opts* opts,
                     uint64_t* class_counts, dm_stats* stats);
 
+/* ---- batched mining (no counterpart in the reference, whose drivers run one graph and one
+   query per process) ----
+   Many (graph, query) pairs run in ONE persistent kernel launch over the disjoint union of
+   their graphs, captured once in a CUDA graph and replayed by dm_batch_run. Every task
+   carries its query; a per-query descriptor selects the path (clique bitmap/list, motif
+   with virtual-warp width 8/16/32) and the donation trigger. */
+#define DM_QUERY_CLIQUE 0
+#define DM_QUERY_MOTIF 1
+#define DM_AUTOTUNE_MODEL 0    /* choose per query from a cost model of the graph */
+#define DM_AUTOTUNE_MEASURE 1  /* time each candidate on the query alone, keep the fastest */
+
+typedef struct dm_query {
+  int32_t kind;                /* DM_QUERY_* */
+  int32_t k;                   /* cliques: [2, 6]; motifs: [3, 5] */
+  dm_graph* graph;
+  const dm_dictionary* dict;   /* motifs: the k-vertex dictionary; cliques: NULL */
+  int32_t vwarp;               /* 0 = autotune, else 8, 16 or 32 (motifs) */
+  int32_t threshold;           /* -1 = autotune, else the dm_opts.threshold meaning */
+  int32_t mode;                /* DM_MODE_AUTO = autotune, DM_MODE_LIST, DM_MODE_BITMAP (cliques) */
+  int32_t reserved;
+} dm_query;
+
+typedef struct dm_query_tuning {
+  int32_t vwarp;               /* chosen virtual-warp width (cliques: 32) */
+  int32_t threshold;           /* chosen donation threshold (100 = no donation) */
+  int32_t mode;                /* DM_MODE_LIST / DM_MODE_BITMAP (motifs: DM_MODE_LIST) */
+  int32_t n_results;           /* 1 (cliques) or the dictionary's class count (motifs) */
+  int64_t result_offset;       /* first result of this query in dm_batch_run's output */
+  double tune_ms;              /* measured time of the chosen setting (DM_AUTOTUNE_MEASURE), else 0 */
+  double est_cost;             /* cost-model estimate of the query's work (arbitrary units) */
+} dm_query_tuning;
+
+typedef struct dm_batch dm_batch;
+
+/* Builds the union graph and descriptor table on the device, tunes every query and
+   captures the launch. opts: device, threads, donations_per_warp, timeout_ms as in
+   dm_count_cliques (may be NULL). The graphs must stay alive until dm_batch_free. */
+DM_API int dm_batch_create(const dm_query* queries, int32_t n_queries, const dm_opts* opts, int32_t autotune,
+                           dm_batch** out);
+/* Total result words (sum of n_results over the queries). */
+DM_API int64_t dm_batch_num_results(const dm_batch* b);
+DM_API int dm_batch_tuning(const dm_batch* b, int32_t query, dm_query_tuning* out);
+/* Replays the captured launch: results[result_offset(q) ..] receives query q's count(s). */
+DM_API int dm_batch_run(dm_batch* b, uint64_t* results, int64_t n_results, dm_stats* stats);
+DM_API void dm_batch_free(dm_batch* b);
+
 /* Work model of the clique path (host-side, for roofline accounting only; it is not a
    counting path): on the degree-ordered DAG, every DFS node at levels 0..k-2 that computes
    a candidate set C_child = C_parent cap N+(v) costs 4(|C_parent| + |N+(v)|) + 4|C_child|
