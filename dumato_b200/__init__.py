@@ -408,7 +408,7 @@ class Options:
     stream: int = 0
     threads: int = 0
     block_size: int = 0
-    donations_per_warp: int = 16
+    donations_per_warp: int = 0
     threshold: int = 0
     vwarp: int = 0
     mode: int = MODE_AUTO

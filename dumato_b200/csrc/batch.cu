@@ -59,8 +59,11 @@ struct BatchArgs {
 constexpr int BATCH_WARPS = 8;
 constexpr int BATCH_CLIQUE_KMAX = 6;
 constexpr int BATCH_MOTIF_KMAX = 5;
-// bitmap rows of up to 4 words (out-degree 256) for every clique query of a batch
-constexpr int BATCH_M = 4;
+// bitmap rows of up to 2 words: clique roots with out-degree up to 128 take the bitmap path,
+// larger ones the list path. The per-warp shared memory then stays small enough for four
+// blocks per SM (the motif paths, which dominate mixed batches, are latency-bound and want
+// the resident warps).
+constexpr int BATCH_M = 2;
 
 template <int M>
 __host__ __device__ constexpr size_t batch_warp_smem() {
@@ -132,7 +135,7 @@ __global__ void batch_reset(DevCounters* c, int n_roots) {
 }
 
 template <int M>
-__global__ void __launch_bounds__(32 * BATCH_WARPS) batch_kernel(BatchArgs a) {
+__global__ void __launch_bounds__(32 * BATCH_WARPS, 4) batch_kernel(BatchArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int lane = lane_id();
   const int wib = warp_in_block();
@@ -386,7 +389,7 @@ int dm_batch_create(const dm_query* queries, int32_t n, const dm_opts* opts, int
   std::vector<int32_t> hrow, pdeg, padj;
   std::vector<std::pair<double, int32_t>> roots;  // (cost, global id)
   std::vector<BatchQuery> desc((size_t)n);
-  std::vector<double> qcost((size_t)n, 0.0), qmax((size_t)n, 0.0);
+  std::vector<double> qcost((size_t)n, 0.0);
   int64_t total_v = 0;
   for (int32_t i = 0; i < n; ++i) {
     const dm_query& q = queries[i];
@@ -424,7 +427,6 @@ int dm_batch_create(const dm_query* queries, int32_t n, const dm_opts* opts, int
         }
       }
       qcost[i] += c;
-      qmax[i] = std::max(qmax[i], c);
     }
     BatchQuery& d = desc[i];
     std::memset(&d, 0, sizeof(d));
@@ -437,9 +439,6 @@ int dm_batch_create(const dm_query* queries, int32_t n, const dm_opts* opts, int
     total_v += g->n;
   }
   vbase[n] = (int32_t)total_v;
-  double total_cost = 0;
-  for (double c : qcost) total_cost += c;
-  const int total_warps_est = ctx.num_sms * 32;
 
   // ---- autotuning ----
   int64_t off = 0;
@@ -449,16 +448,16 @@ int dm_batch_create(const dm_query* queries, int32_t n, const dm_opts* opts, int
     dm_query_tuning& t = b->tuning[i];
     const bool clique = q.kind == DM_QUERY_CLIQUE;
     t.est_cost = qcost[i];
-    // cost model: bitmap intersection wherever a root's out-neighbourhood fits 256 bits (the
-    // list path takes the larger roots); narrow groups only pay off when the extension sets
-    // are tiny (k = 3 on a sparse graph); donate only from queries whose heaviest root
-    // exceeds a warp's fair share of the whole batch
-    int vw = 32, thr = 100, mode = clique ? DM_MODE_AUTO : DM_MODE_LIST;
+    // cost model: bitmap intersection wherever a root's out-neighbourhood fits the bitmap
+    // rows (the list path takes the larger roots); narrow groups only pay off when the
+    // extension sets are tiny (k = 3 on a sparse graph); every query donates on demand
+    // (threshold 0): donation is demand-limited, so it costs nothing while no warp is
+    // hungry, and a per-root estimate that is too low must not leave a heavy root unsplit
+    int vw = 32, thr = 0, mode = clique ? DM_MODE_AUTO : DM_MODE_LIST;
     if (!clique) {
       const double mean_deg = q.graph->n ? 2.0 * (double)q.graph->m / q.graph->n : 0.0;
       if (q.k == 3 && mean_deg <= 16.0) vw = 16;
     }
-    if (qmax[i] > total_cost / std::max(1, total_warps_est)) thr = 0;
     if (autotune == DM_AUTOTUNE_MEASURE) {
       const std::vector<int> vws = clique ? std::vector<int>{32} : std::vector<int>{8, 16, 32};
       const std::vector<int> modes = clique ? std::vector<int>{DM_MODE_AUTO, DM_MODE_LIST} : std::vector<int>{DM_MODE_AUTO};

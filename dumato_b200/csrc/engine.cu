@@ -137,7 +137,7 @@ int select_device(const dm_opts* o, LaunchCtx& ctx) {
     ctx.block = o->block_size;
     ctx.vwarp = o->vwarp;
     ctx.threshold = o->threshold > 0 ? o->threshold : 0;
-    ctx.donations_per_warp = o->donations_per_warp > 0 ? o->donations_per_warp : 16;
+    ctx.donations_per_warp = o->donations_per_warp > 0 ? o->donations_per_warp : 64;
     ctx.test_stall = (o->test_flags & DM_TEST_STALL_AT_EXIT) ? 1 : 0;
     if (o->test_flags & DM_TEST_EAGER_DONATION) ctx.donate_after_us = 0;
   }

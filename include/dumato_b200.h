@@ -94,7 +94,7 @@ typedef struct dm_opts {
   uint64_t stream;             /* cudaStream_t to launch on; 0 = the library's own stream */
   int32_t threads;             /* reference argv[3]: total GPU threads (0 = persistent default) */
   int32_t block_size;          /* reference argv[4]: threads per block (0 = 256) */
-  int32_t donations_per_warp;  /* reference argv[5]: donation batch bound (0 = 16) */
+  int32_t donations_per_warp;  /* reference argv[5]: donations one task may make (0 = 64) */
   int32_t threshold;           /* reference argv[6]: idle-warp percentage that triggers donation;
                                   >= 100 disables donation (clique_PA.cu:78) */
   int32_t vwarp;               /* virtual-warp width 0 (auto), 8, 16 or 32 */
