@@ -144,10 +144,41 @@ int select_device(const dm_opts* o, LaunchCtx& ctx) {
   return DM_OK;
 }
 
+// Workspaces of released graphs, per device, handed to the next graph that needs one on that
+// device. A graph's own device memory is its CSR copies and root orders; the scratch, the
+// donation queue, the counters and the events are not tied to a graph, and allocating and
+// freeing them costs milliseconds per call that re-uploads a graph.
+static std::map<int, std::vector<Workspace>> g_ws_pool;
+constexpr size_t WS_POOL_MAX = 4;
+
+static void free_workspace(Workspace& w) {
+  cudaFree(w.d_ctr);
+  cudaFree(w.d_tasks);
+  cudaFree(w.d_scratch);
+  cudaFree(w.d_hist);
+  cudaFree(w.d_q2c);
+  cudaFree(w.d_queue);
+  cudaFree(w.d_per_root);
+  cudaFree(w.d_parts);
+  if (w.ev0) cudaEventDestroy(w.ev0);
+  if (w.ev1) cudaEventDestroy(w.ev1);
+  if (w.k0) cudaEventDestroy(w.k0);
+  if (w.k1) cudaEventDestroy(w.k1);
+  w = Workspace();
+}
+
 static DeviceSlot* slot_for(dm_graph* g, int dev) {
   for (auto* p : g->dev)
     if (p->device == dev) return reinterpret_cast<DeviceSlot*>(p);
   auto* s = new DeviceSlot();
+  {
+    std::lock_guard<std::mutex> lk(g_dev_mu);
+    auto& pool = g_ws_pool[dev];
+    if (!pool.empty()) {
+      s->ws = pool.back();
+      pool.pop_back();
+    }
+  }
   s->dg.device = dev;
   g->dev.push_back(&s->dg);
   return s;
@@ -235,24 +266,21 @@ void release_device_graphs(dm_graph* g) {
       cudaFree(s->dg.d_orow);
       cudaFree(s->dg.d_odeg);
       cudaFree(s->dg.d_oadj);
-      cudaFree(s->ws.d_ctr);
-      cudaFree(s->ws.d_tasks);
-      cudaFree(s->ws.d_scratch);
-      cudaFree(s->ws.d_hist);
-      cudaFree(s->ws.d_q2c);
-      cudaFree(s->ws.d_queue);
-      cudaFree(s->ws.d_per_root);
-      cudaFree(s->ws.d_parts);
+      {
+        std::lock_guard<std::mutex> lk(g_dev_mu);
+        auto& pool = g_ws_pool[s->dg.device];
+        if (s->ws.d_queue && pool.size() < WS_POOL_MAX) {
+          pool.push_back(s->ws);
+          s->ws = Workspace();
+        }
+      }
+      free_workspace(s->ws);
       cudaFree(s->d_deg_order);
       cudaFree(s->d_up_order);
       for (auto& l : s->learned) {
         cudaFree(l.d_roots);
         cudaFree(l.d_parts);
       }
-      if (s->ws.ev0) cudaEventDestroy(s->ws.ev0);
-      if (s->ws.ev1) cudaEventDestroy(s->ws.ev1);
-      if (s->ws.k0) cudaEventDestroy(s->ws.k0);
-      if (s->ws.k1) cudaEventDestroy(s->ws.k1);
       cudaSetDevice(cur);
     }
     cudaGetLastError();
