@@ -24,37 +24,6 @@ def make(name: str, seed: int = 1):
     return Graph.generate(kind, p.pop("n"), p.pop("m"), seed=seed, **p)
 
 
-def main(argv=None) -> int:
-    """Runs one query on a named workload `reps` times and prints the last run's count and
-    kernel time (the command line the kernel profiles are taken with)."""
-    import argparse
-
-    from . import Dictionary, count_cliques, count_motifs
-
-    ap = argparse.ArgumentParser(prog="python -m dumato_b200.workloads")
-    ap.add_argument("query", choices=("clique", "motif"))
-    ap.add_argument("workload", choices=sorted(CONFIGS))
-    ap.add_argument("k", type=int)
-    ap.add_argument("--reps", type=int, default=2)
-    ap.add_argument("--seed", type=int, default=1)
-    args = ap.parse_args(argv)
-    g = make(args.workload, args.seed)
-    d = Dictionary.generate(args.k) if args.query == "motif" else None
-    for _ in range(max(1, args.reps)):
-        if d is None:
-            total, st = count_cliques(g, args.k)
-        else:
-            hist, st = count_motifs(g, args.k, d)
-            total = int(hist.sum())
-    print(f"{args.query} {args.workload} k={args.k}: {total} in {st.kernel_ms:.3f} ms "
-          f"(tasks {st.tasks}, donations {st.donations}, prefix donations {st.prefix_donations})")
-    return 0
-
-
-if __name__ == "__main__":
-    raise SystemExit(main())
-
-
 # Batched-mining workload: graphs of uneven size, one query each.
 BATCH_QUERIES = [("clique", 3), ("clique", 4), ("clique", 5), ("clique", 6), ("motif", 3), ("motif", 4), ("motif", 5)]
 
@@ -110,9 +79,10 @@ def main(argv=None) -> int:
     ap.add_argument("k", type=int, nargs="?", default=4)
     ap.add_argument("--reps", type=int, default=2)
     ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--graphs", type=int, default=256, help="batch: number of graphs")
     args = ap.parse_args(argv)
     if args.query == "batch":
-        queries, _graphs, _dicts = make_batch(args.seed)
+        queries, _graphs, _dicts = make_batch(args.seed, args.graphs)
         b = Batch(queries)
         for _ in range(max(1, args.reps)):
             res, st = b.run()
