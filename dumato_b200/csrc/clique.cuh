@@ -126,7 +126,8 @@ struct CliqueArgs {
 
 // Loads L = N+(root) into shared memory and the exclusive prefix sum of the out-degrees
 // of its members (sP[0..d]). Returns the total.
-static __device__ __forceinline__ int load_root_list(const GraphView& g, int root, int d, int32_t* sL, int32_t* sP) {
+static __device__ __forceinline__ int load_root_list(const GraphView& g, int root, int d, int32_t* sL, int32_t* sP,
+                                                     int32_t* sR) {
   const int lane = lane_id();
   const int32_t* L = g.adj + __ldg(g.row + root);
   int carry = 0;
@@ -136,6 +137,7 @@ static __device__ __forceinline__ int load_root_list(const GraphView& g, int roo
     if (i < d) {
       u = __ldg(L + i);
       du = __ldg(g.deg + u);
+      sR[i] = __ldg(g.row + u);
       sL[i] = u;
     }
     int s = du;
@@ -154,17 +156,37 @@ static __device__ __forceinline__ int load_root_list(const GraphView& g, int roo
 
 // Local adjacency bitmap of L (rows zeroed by the caller): the (member, out-neighbour)
 // pairs are flattened so the warp stays busy when rows are short; membership in L is a
-// binary search in shared memory.
-static __device__ __forceinline__ void build_local_rows(const GraphView& g, const int32_t* sL, const int32_t* sP, int d,
-                                                 int total, uint32_t* rows, int row_words) {
+// binary search in shared memory. Row starts come from shared memory (sR, filled with L), and
+// each lane issues the loads of BUILD_UNROLL pairs before it uses any of them, so the
+// adjacency loads of a lane overlap instead of forming one dependent chain per pair.
+constexpr int BUILD_UNROLL = 4;
+
+static __device__ __forceinline__ void build_local_rows(const int32_t* adj, const int32_t* sL, const int32_t* sP,
+                                                        const int32_t* sR, int d, int total, uint32_t* rows,
+                                                        int row_words) {
   const int lane = lane_id();
   const int32_t maxL = sL[d - 1];
-  for (int f = lane; f < total; f += 32) {
-    const int i = lower_bound(sP, 0, d + 1, f + 1) - 1;  // largest i with sP[i] <= f
-    const int32_t x = __ldg(g.adj + __ldg(g.row + sL[i]) + (f - sP[i]));
-    if (x <= maxL) {
-      const int j = lower_bound(sL, i + 1, d, x);
-      if (j < d && sL[j] == x) atomicOr(rows + i * row_words + (j >> 5), 1u << (j & 31));
+  int i = 0;  // member owning pair f: the largest i with sP[i] <= f (f only grows per lane)
+  for (int f0 = lane; f0 < total; f0 += 32 * BUILD_UNROLL) {
+    int32_t x[BUILD_UNROLL];
+    int own[BUILD_UNROLL];
+#pragma unroll
+    for (int u = 0; u < BUILD_UNROLL; ++u) {
+      const int f = f0 + 32 * u;
+      own[u] = -1;
+      if (f < total) {
+        while (sP[i + 1] <= f) ++i;
+        own[u] = i;
+        x[u] = __ldg(adj + sR[i] + (f - sP[i]));
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < BUILD_UNROLL; ++u) {
+      const int m = own[u];
+      if (m >= 0 && x[u] <= maxL) {
+        const int j = lower_bound(sL, m + 1, d, x[u]);
+        if (j < d && sL[j] == x[u]) atomicOr(rows + m * row_words + (j >> 5), 1u << (j & 31));
+      }
     }
   }
 }
@@ -255,8 +277,9 @@ __device__ unsigned long long bitmap_task(const CliqueArgs& a, unsigned char* ws
   int* heavy = reinterpret_cast<int*>(wsm + LY.heavy);
   const long long t_start = global_ns();
   for (int i = lane; i < d * RW; i += 32) rows32[i] = 0;
-  const int total = load_root_list(a.g, root, d, sL, sP);
-  build_local_rows(a.g, sL, sP, d, total, rows32, RW);
+  // sE holds the members' row starts while the rows are built, the item prefix after
+  const int total = load_root_list(a.g, root, d, sL, sP, sE);
+  build_local_rows(a.g.adj, sL, sP, sE, d, total, rows32, RW);
   __syncwarp();
   const uint64_t* rows = reinterpret_cast<const uint64_t*>(rows32);
   int n_items;
