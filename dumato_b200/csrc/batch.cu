@@ -39,7 +39,7 @@ struct BatchQuery {
   int arena_stride;     // motifs: int2 slots per group
   int arena_dcap;       // cliques: list capacity per level
   int n_classes;
-  int pad;
+  int bit_words;        // motifs: membership bitmap words (0 = none)
   const int32_t* q2c;   // motifs: quick code -> class
   unsigned long long* out;  // count (cliques) or class counters (motifs)
 };
@@ -54,6 +54,8 @@ struct BatchArgs {
   int n_queries;
   unsigned char* arena;
   size_t arena_bytes;          // per warp
+  uint32_t* bits;              // motif membership bitmaps (zero between runs), or null
+  size_t bits_words;           // per warp
 };
 
 constexpr int BATCH_WARPS = 8;
@@ -100,8 +102,9 @@ __device__ unsigned long long batch_clique(const BatchArgs& a, const BatchQuery&
 }
 
 template <int K, int W>
-__device__ void batch_motif(const BatchArgs& a, const BatchQuery& q, unsigned char* wsm, int2* arena, int v0, int b,
-                            int e, int level, const int* path, unsigned long long& nodes) {
+__device__ void batch_motif(const BatchArgs& a, const BatchQuery& q, unsigned char* wsm, int2* arena,
+                            uint32_t* bits, int v0, int b, int e, int level, const int* path,
+                            unsigned long long& nodes) {
   MotifCtx c;
   c.g = a.g;
   c.lb = a.lb;
@@ -111,20 +114,23 @@ __device__ void batch_motif(const BatchArgs& a, const BatchQuery& q, unsigned ch
   c.maxdeg = q.maxdeg;
   c.arena_stride = q.arena_stride;
   c.per_root = nullptr;
+  c.bit_base = q.vbase;
+  c.bit_words = bits ? q.bit_words : 0;
   MotifShared* ws = reinterpret_cast<MotifShared*>(wsm);
   MotifGroup* groups = reinterpret_cast<MotifGroup*>(ws + 1);
   unsigned long long tn = 0;
-  motif_run_task<K, W>(c, q.out, ws, groups, arena, v0, b, e, level, path, tn);
+  motif_run_task<K, W>(c, q.out, ws, groups, arena, bits, v0, b, e, level, path, tn);
   // every lane of a group counted the group's nodes: keep the leaders' counts
   if ((lane_id() & (W - 1)) == 0) nodes += tn;
 }
 
 template <int K>
-__device__ void batch_motif_w(const BatchArgs& a, const BatchQuery& q, unsigned char* wsm, int2* arena, int v0,
-                              int b, int e, int level, const int* path, unsigned long long& nodes) {
-  if (q.vwarp == 8) batch_motif<K, 8>(a, q, wsm, arena, v0, b, e, level, path, nodes);
-  else if (q.vwarp == 16) batch_motif<K, 16>(a, q, wsm, arena, v0, b, e, level, path, nodes);
-  else batch_motif<K, 32>(a, q, wsm, arena, v0, b, e, level, path, nodes);
+__device__ void batch_motif_w(const BatchArgs& a, const BatchQuery& q, unsigned char* wsm, int2* arena,
+                              uint32_t* bits, int v0, int b, int e, int level, const int* path,
+                              unsigned long long& nodes) {
+  if (q.vwarp == 8) batch_motif<K, 8>(a, q, wsm, arena, bits, v0, b, e, level, path, nodes);
+  else if (q.vwarp == 16) batch_motif<K, 16>(a, q, wsm, arena, bits, v0, b, e, level, path, nodes);
+  else batch_motif<K, 32>(a, q, wsm, arena, bits, v0, b, e, level, path, nodes);
 }
 
 __global__ void batch_reset(DevCounters* c, int n_roots) {
@@ -143,6 +149,7 @@ __global__ void __launch_bounds__(32 * BATCH_WARPS, 4) batch_kernel(BatchArgs a)
   const size_t gw = (size_t)blockIdx.x * BATCH_WARPS + wib;
   const int total_warps = gridDim.x * BATCH_WARPS;
   unsigned char* warp_arena = a.arena + gw * a.arena_bytes;
+  uint32_t* warp_bits = a.bits ? a.bits + gw * a.bits_words : nullptr;
   unsigned long long ntasks = 0, nodes = 0;
   while (true) {
     int first = 0, count = 0, b = 0, e = -1, ok = 0, level = 0;
@@ -189,9 +196,9 @@ __global__ void __launch_bounds__(32 * BATCH_WARPS, 4) batch_kernel(BatchArgs a)
           if (lane == 0) set_err(a.lb.ctr, ERR_BAD_TASK);
         } else {
           switch (k) {
-            case 3: batch_motif_w<3>(a, q, wsm, arena, root, b, e, level, path, nodes); break;
-            case 4: batch_motif_w<4>(a, q, wsm, arena, root, b, e, level, path, nodes); break;
-            case 5: batch_motif_w<5>(a, q, wsm, arena, root, b, e, level, path, nodes); break;
+            case 3: batch_motif_w<3>(a, q, wsm, arena, warp_bits, root, b, e, level, path, nodes); break;
+            case 4: batch_motif_w<4>(a, q, wsm, arena, warp_bits, root, b, e, level, path, nodes); break;
+            case 5: batch_motif_w<5>(a, q, wsm, arena, warp_bits, root, b, e, level, path, nodes); break;
             default:
               if (lane == 0) set_err(a.lb.ctr, ERR_BAD_TASK);
           }
@@ -253,6 +260,8 @@ struct dm_batch {
   DevCounters* d_ctr = nullptr;
   void* d_queue = nullptr;
   unsigned char* d_arena = nullptr;
+  uint32_t* d_bits = nullptr;
+  size_t bits_bytes = 0;
   std::map<uint64_t, int32_t*> d_q2c;  // per dictionary uid
   unsigned long long* h_out = nullptr;  // pinned
   DevCounters* h_ctr = nullptr;         // pinned
@@ -282,6 +291,7 @@ void batch_release(dm_batch* b) {
     cudaFree(b->d_ctr);
     cudaFree(b->d_queue);
     cudaFree(b->d_arena);
+    cudaFree(b->d_bits);
     for (auto& kv : b->d_q2c) cudaFree(kv.second);
     if (b->h_out) cudaFreeHost(b->h_out);
     if (b->h_ctr) cudaFreeHost(b->h_ctr);
@@ -494,6 +504,7 @@ int dm_batch_create(const dm_query* queries, int32_t n, const dm_opts* opts, int
       d.arena_dcap = d.maxdeg + 4;
     } else {
       d.arena_stride = (int)motif_group_stride(q.k, d.maxdeg);
+      d.bit_words = motif_bit_words(d.nv);
     }
   }
   b->n_results = off;
@@ -568,6 +579,19 @@ int dm_batch_create(const dm_query* queries, int32_t n, const dm_opts* opts, int
   ce = cudaMalloc(&b->d_arena, arena_bytes * (size_t)warps);
   if (ce != cudaSuccess)
     return fail_release(b, fail(DM_ECUDA, std::string("dm_batch_create: arena: ") + cudaGetErrorString(ce)));
+  // membership bitmaps of the motif queries: per warp, 32/W groups x 2 bitmaps over the
+  // largest motif graph (zeroed here; every task leaves them zero)
+  size_t bits_words = 0;
+  for (int32_t i = 0; i < n; ++i)
+    if (desc[i].kind == DM_QUERY_MOTIF)
+      bits_words = std::max(bits_words, (size_t)desc[i].bit_words * 2 * (32 / desc[i].vwarp));
+  if (bits_words && bits_words * sizeof(uint32_t) * (size_t)warps <= ((size_t)2 << 30)) {
+    b->bits_bytes = bits_words * sizeof(uint32_t) * (size_t)warps;
+    ce = cudaMalloc(&b->d_bits, b->bits_bytes);
+    if (ce == cudaSuccess) ce = cudaMemsetAsync(b->d_bits, 0, b->bits_bytes, b->stream);
+    if (ce != cudaSuccess)
+      return fail_release(b, fail(DM_ECUDA, std::string("dm_batch_create: bitmaps: ") + cudaGetErrorString(ce)));
+  }
   if ((rc = upload(reinterpret_cast<void**>(&b->d_desc), desc.data(), sizeof(BatchQuery) * desc.size())))
     return fail_release(b, rc);
   DM_CUDA(cudaStreamSynchronize(b->stream));
@@ -585,6 +609,8 @@ int dm_batch_create(const dm_query* queries, int32_t n, const dm_opts* opts, int
   a.n_queries = n;
   a.arena = b->d_arena;
   a.arena_bytes = arena_bytes;
+  a.bits = b->d_bits;
+  a.bits_words = bits_words;
 
   // ---- capture: reset, clear, launch, read back ----
   ce = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
@@ -626,6 +652,7 @@ int dm_batch_run(dm_batch* b, uint64_t* results, int64_t n_results, dm_stats* st
   if (h.err) {
     // a failed launch can leave donations queued: empty the queue for the next run
     queue_init_launch(b->d_queue, QUEUE_SHARDS, QUEUE_SHARD_SLOTS, b->stream);
+    if (b->d_bits) cudaMemsetAsync(b->d_bits, 0, b->bits_bytes, b->stream);
     cudaStreamSynchronize(b->stream);
     return fail(h.err == ERR_TIMEOUT ? DM_ETIMEOUT : DM_EOVERFLOW, "batch kernel reported error " + std::to_string(h.err));
   }

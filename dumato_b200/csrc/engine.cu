@@ -42,6 +42,8 @@ struct Workspace {
   size_t per_root_cap = 0;
   int32_t* d_parts = nullptr;       // scheduler part words, parallel to the task list
   size_t parts_cap = 0;
+  uint32_t* d_bits = nullptr;       // motif membership bitmaps, all zero between calls
+  size_t bits_cap = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, k0 = nullptr, k1 = nullptr;
 };
 
@@ -160,6 +162,7 @@ static void free_workspace(Workspace& w) {
   cudaFree(w.d_queue);
   cudaFree(w.d_per_root);
   cudaFree(w.d_parts);
+  cudaFree(w.d_bits);
   if (w.ev0) cudaEventDestroy(w.ev0);
   if (w.ev1) cudaEventDestroy(w.ev1);
   if (w.k0) cudaEventDestroy(w.k0);
@@ -684,6 +687,21 @@ int dm_count_motifs(dm_graph* g, int32_t k, const dm_dictionary* dict, const dm_
   const size_t budget = (size_t)8 << 30;
   ctx.arena_warps = (int)std::min<size_t>((size_t)ctx.num_sms * 64, std::max<size_t>(8, budget / per_warp));
   if ((rc = ensure_ws_bytes(&ws.d_scratch, &ws.scratch_cap, per_warp * ctx.arena_warps))) return rc;
+  // membership bitmaps (2 per group, zero between calls; skipped past 2 GB)
+  const int bit_words = motif_bit_words(g->n);
+  const size_t bits_bytes = (size_t)bit_words * 2 * (32 / vwarp) * sizeof(uint32_t) * ctx.arena_warps;
+  uint32_t* d_bits = nullptr;
+  if (bits_bytes <= ((size_t)2 << 30)) {
+    if (ws.bits_cap < bits_bytes) {
+      cudaFree(ws.d_bits);
+      ws.d_bits = nullptr;
+      ws.bits_cap = 0;
+      DM_CUDA(cudaMalloc(&ws.d_bits, bits_bytes));
+      DM_CUDA(cudaMemsetAsync(ws.d_bits, 0, bits_bytes, ctx.stream));
+      ws.bits_cap = bits_bytes;
+    }
+    d_bits = ws.d_bits;
+  }
   const bool want_log = o && o->subtree_counts;
   if (want_log) {
     if ((rc = ensure_ws_bytes(reinterpret_cast<void**>(&ws.d_per_root), &ws.per_root_cap,
@@ -712,6 +730,8 @@ int dm_count_motifs(dm_graph* g, int32_t k, const dm_dictionary* dict, const dm_
   L.maxdeg = maxdeg;
   L.per_root = want_log ? ws.d_per_root : nullptr;
   L.vwarp = vwarp;
+  L.bits = d_bits;
+  L.bit_words = bit_words;
   DM_CUDA(cudaEventRecord(ws.k0, ctx.stream));
   int grid = 0;
   if (n_roots > 0) {
@@ -727,6 +747,11 @@ int dm_count_motifs(dm_graph* g, int32_t k, const dm_dictionary* dict, const dm_
     DM_CUDA(cudaMemcpyAsync(o->subtree_counts, ws.d_per_root, sizeof(unsigned long long) * g->n,
                             cudaMemcpyDeviceToHost, ctx.stream));
   DM_CUDA(cudaStreamSynchronize(ctx.stream));
+  if (h.err && d_bits) {
+    // a failed launch can leave bits set: clear them for the next call
+    DM_CUDA(cudaMemsetAsync(ws.d_bits, 0, ws.bits_cap, ctx.stream));
+    DM_CUDA(cudaStreamSynchronize(ctx.stream));
+  }
   if ((rc = reset_queue(ws, h, ctx.stream))) return rc;
   float kms = 0, pms = 0;
   cudaEventElapsedTime(&kms, ws.k0, ws.k1);

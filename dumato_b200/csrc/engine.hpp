@@ -105,7 +105,11 @@ struct MotifLaunch {
   unsigned long long* per_root = nullptr;
   const int32_t* parts = nullptr;
   int vwarp = 32;                // virtual-warp width: 8, 16 or 32
+  uint32_t* bits = nullptr;      // per warp: 32/vwarp x 2 zeroed bitmaps of bit_words words (or null)
+  int bit_words = 0;
 };
+// 32-bit words of one membership bitmap over n vertices.
+inline int motif_bit_words(int n) { return (n + 31) / 32 + 1; }
 int motif_launch(const MotifLaunch& L, LaunchCtx& ctx, int* grid);
 size_t motif_arena_stride(int k, int maxdeg, int vwarp);  // int2 slots per warp
 

@@ -19,6 +19,7 @@ struct MotifArgs {
   int n_classes;
   unsigned long long* hist;    // n_classes
   int2* arena;                 // per warp: 32/W group arenas of c.arena_stride int2
+  uint32_t* bits;              // per warp: 32/W groups x 2 membership bitmaps of c.bit_words (or null)
   const int32_t* parts;        // optional per-root-entry part word (p | P << 16)
 };
 
@@ -37,6 +38,7 @@ __global__ void __launch_bounds__(32 * MOTIF_WARPS, 4) motif_kernel(MotifArgs a)
   const size_t gw = (size_t)blockIdx.x * MOTIF_WARPS + wib;
   const int total_warps = gridDim.x * MOTIF_WARPS;
   int2* warp_arena = a.arena + gw * (size_t)c.arena_stride * (32 / W);
+  uint32_t* warp_bits = a.bits ? a.bits + gw * (size_t)c.bit_words * 2 * (32 / W) : nullptr;
   unsigned long long ntasks = 0, nodes = 0;
   while (true) {
     int first = 0, count = 0, b = 0, e = -1, ok = 0, level = 0;
@@ -67,7 +69,7 @@ __global__ void __launch_bounds__(32 * MOTIF_WARPS, 4) motif_kernel(MotifArgs a)
       if (!donated && a.parts) part_bounds(__ldg(a.parts + first + ti), bb, ee);
       ++ntasks;
       // block-level class counters, added to the global ones at exit
-      motif_run_task<K, W>(c, bhist, ws, groups, warp_arena, v0, bb, ee, level, path, nodes);
+      motif_run_task<K, W>(c, bhist, ws, groups, warp_arena, warp_bits, v0, bb, ee, level, path, nodes);
     }
     if (lane == 0) lb_done(c.lb, count);
   }
@@ -129,6 +131,9 @@ int motif_launch(const MotifLaunch& L, LaunchCtx& ctx, int* grid) {
   a.c.maxdeg = L.maxdeg;
   a.c.arena_stride = (int)motif_group_stride(L.k, L.maxdeg);
   a.c.per_root = L.per_root;
+  a.c.bit_base = 0;
+  a.c.bit_words = L.bits ? L.bit_words : 0;
+  a.bits = L.bits;
   a.roots = L.roots;
   a.n_roots = L.n_roots;
   a.n_classes = L.n_classes;

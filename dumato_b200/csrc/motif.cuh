@@ -81,7 +81,33 @@ struct MotifCtx {
   int maxdeg;                  // bound on every degree in g (arena sizing)
   int arena_stride;            // int2 slots per group
   unsigned long long* per_root;  // optional: subgraphs found under each v0 (subtree logger)
+  int bit_base;                // membership bitmaps index vertex x at bit x - bit_base
+  int bit_words;               // 32-bit words per bitmap (0 = no bitmaps: binary searches only)
 };
+
+// Membership bitmaps of one group (2 x bit_words words in global memory, all zero between
+// tasks): U holds U_t = N(v_0..v_t) above v0 for the levels materialised on the current path,
+// E holds E_{k-3} (k = 3: E_0). They turn the leaf step and the exclusion test into one probe
+// per neighbour instead of binary searches over the runs.
+__device__ __forceinline__ bool bit_test(const uint32_t* b, int x) { return (b[x >> 5] >> (x & 31)) & 1u; }
+
+template <int W>
+__device__ __forceinline__ void bits_flip_ids(uint32_t* b, int base, const int32_t* ids, int n, bool set, int gl) {
+  for (int i = gl; i < n; i += W) {
+    const int x = __ldg(ids + i) - base;
+    if (set) atomicOr(b + (x >> 5), 1u << (x & 31));
+    else atomicAnd(b + (x >> 5), ~(1u << (x & 31)));
+  }
+}
+
+template <int W>
+__device__ __forceinline__ void bits_flip_list(uint32_t* b, int base, const int2* list, int n, bool set, int gl) {
+  for (int i = gl; i < n; i += W) {
+    const int x = list[i].x - base;
+    if (set) atomicOr(b + (x >> 5), 1u << (x & 31));
+    else atomicAnd(b + (x >> 5), ~(1u << (x & 31)));
+  }
+}
 
 // int2 slots of one group's arena: extension levels 1..k-3 (level t holds at most
 // (t+1) * maxdeg members) then runs 1..k-3 (at most maxdeg each).
@@ -199,8 +225,9 @@ __device__ __forceinline__ void motif_try_donate(const LBArgs& lb, MotifShared* 
 // lane of a group counts the same nodes; the caller keeps group leaders' counts only).
 template <int K, int W>
 __device__ __forceinline__ void motif_run_task(const MotifCtx& c, unsigned long long* hist, MotifShared* ws,
-                                               MotifGroup* groups, int2* warp_arena, int v0, int bb, int ee,
-                                               int level, const int* path, unsigned long long& nodes) {
+                                               MotifGroup* groups, int2* warp_arena, uint32_t* warp_bits, int v0,
+                                               int bb, int ee, int level, const int* path,
+                                               unsigned long long& nodes) {
   static_assert(W == 8 || W == 16 || W == 32, "virtual warp width must be 8, 16 or 32");
   const int lane = lane_id();
   const int gl = lane & (W - 1);
@@ -216,6 +243,10 @@ __device__ __forceinline__ void motif_run_task(const MotifCtx& c, unsigned long 
   int2* const runs1 = ext_at(K - 2);
   const size_t rstride = md + 32;
   auto run_at = [&](int t) -> int2* { return runs1 + (size_t)(t - 1) * rstride; };
+  const bool use_bits = warp_bits != nullptr && c.bit_words > 0;
+  uint32_t* const Ub = use_bits ? warp_bits + (size_t)gi * 2 * c.bit_words : nullptr;
+  uint32_t* const Eb = use_bits ? Ub + c.bit_words : nullptr;
+  int bdepth = 0;  // levels 1..bdepth have their run (and, at level k-3, E) bits set
   unsigned long long task_cnt = 0;
   const long long t_start = global_ns();
   // E_0 = run 0 = N(v0) above v0: a suffix of the sorted CSR row
@@ -238,7 +269,20 @@ __device__ __forceinline__ void motif_run_task(const MotifCtx& c, unsigned long 
     sg->spill_lo = sg->spill_hi = 0;
   }
   for (int m = gl; m < 64; m += W) sg->mh[m] = 0;
+  if (use_bits) {
+    bits_flip_ids<W>(Ub, c.bit_base, E0, n0, true, gl);
+    if (K == 3) bits_flip_ids<W>(Eb, c.bit_base, E0, n0, true, gl);
+  }
   __syncwarp();
+  // drops the bits of levels from..bdepth (the group's lanes, then a group barrier)
+  auto drop_levels = [&](int from) {
+    for (int L = bdepth; L >= from; --L) {
+      bits_flip_list<W>(Ub, c.bit_base, run_at(L), sg->runn[L], false, gl);
+      if (L == K - 3) bits_flip_list<W>(Eb, c.bit_base, ext_at(L), sg->n[L], false, gl);
+    }
+    if (bdepth >= from) bdepth = from - 1;
+    __syncwarp(gmask);
+  };
   bool replay_item = level > 0 && gi == 0;
   while (true) {
     int it = 0;
@@ -293,6 +337,40 @@ __device__ __forceinline__ void motif_run_task(const MotifCtx& c, unsigned long 
         // leaves: histogram the masks of E_{p} without writing it
         const int leaf_off = quick_off(K - 1);
         const int n_inh = nE - startE;
+        const int sw0 = lower_bound(Nw, 0, dw, v0 + 1);
+        const int above = dw - sw0;
+        int usize = n0;
+        for (int i = 1; i <= t; ++i) usize += sg->runn[i];
+        if (use_bits && above <= 4 * (n_inh + usize) + 128) {
+          // one pass over N(w) above v0: a neighbour outside U_t is a new member of E_{p}
+          // (excl(w)); a neighbour in E_t above w is an inherited member adjacent to w; the
+          // inherited members not adjacent to w come from the suffix's mask counts
+          if (t == 0) {
+            if (gl == 0 && n_inh) atomicAdd(&sg->mh[1], (unsigned)n_inh);
+          } else {
+            for (int m = gl; m < (1 << (K - 2)); m += W) {
+              const unsigned cm = sg->sh[m];
+              if (cm) atomicAdd(&sg->mh[m], cm);
+            }
+          }
+          __syncwarp(gmask);
+          unsigned ex = 0;
+          for (int i = sw0 + gl; i < dw; i += W) {
+            const int32_t x = Nw[i];
+            const int xb = x - c.bit_base;
+            if (!bit_test(Ub, xb)) {
+              ++ex;
+            } else if (x > w && bit_test(Eb, xb)) {
+              const int em = (t == 0) ? 1 : Et[lower_bound2(Et, startE, nE, x)].y;
+              atomicSub(&sg->mh[em], 1u);
+              atomicAdd(&sg->mh[em | (1 << p)], 1u);
+            }
+          }
+          for (int o = W / 2; o > 0; o >>= 1) ex += __shfl_xor_sync(gmask, ex, o);
+          if (gl == 0 && ex) atomicAdd(&sg->mh[1 << p], ex);
+          __syncwarp(gmask);
+          flush_masks<W>(sg, c.q2c, quick_p, leaf_off, hist, task_cnt, gl, gmask);
+        } else {
         const int gt = lower_bound(Nw, 0, dw, w + 1);
         const int dgt = dw - gt;
         // probe each inherited member in N(w), or take the suffix's mask counts and move
@@ -341,10 +419,6 @@ __device__ __forceinline__ void motif_run_task(const MotifCtx& c, unsigned long 
           }
         }
         // excl(w) = N(w) above v0 minus U_t
-        const int sw0 = lower_bound(Nw, 0, dw, v0 + 1);
-        const int above = dw - sw0;
-        int usize = n0;
-        for (int i = 1; i <= t; ++i) usize += sg->runn[i];
         unsigned inter = 0;
         if ((long long)usize <= (long long)above * (t + 1)) {
           // iterate U_t, probe N(w)
@@ -357,7 +431,8 @@ __device__ __forceinline__ void motif_run_task(const MotifCtx& c, unsigned long 
         } else {
           // iterate N(w) above v0, probe the runs
           for (int i = sw0 + gl; i < dw; i += W)
-            inter += in_runs(Nw[i], E0, n0, runs1, rstride, sg->runn, t) ? 1u : 0u;
+            inter += (use_bits ? bit_test(Ub, Nw[i] - c.bit_base)
+                               : in_runs(Nw[i], E0, n0, runs1, rstride, sg->runn, t)) ? 1u : 0u;
         }
         for (int o = W / 2; o > 0; o >>= 1) inter += __shfl_xor_sync(gmask, inter, o);
         if (gl == 0) {
@@ -366,12 +441,14 @@ __device__ __forceinline__ void motif_run_task(const MotifCtx& c, unsigned long 
         }
         __syncwarp(gmask);
         flush_masks<W>(sg, c.q2c, quick_p, leaf_off, hist, task_cnt, gl, gmask);
+        }
       } else {
         // materialise E_{p} = inherited + excl(w), merged by vertex id; excl(w) is also run
         // p. Both parts are sorted and disjoint, so each member's place is its index in its
         // own part plus the number of smaller members of the other part.
         int2* Ep = ext_at(p);
         int2* Rp = run_at(p);
+        if (use_bits) drop_levels(p);  // the previous member's sets at levels >= p
         const int sw0 = lower_bound(Nw, 0, dw, v0 + 1);
         int rn = 0;
         for (int i0 = sw0; i0 < dw; i0 += W) {
@@ -380,7 +457,7 @@ __device__ __forceinline__ void motif_run_task(const MotifCtx& c, unsigned long 
           bool nw = false;
           if (i < dw) {
             x = Nw[i];
-            nw = !in_runs(x, E0, n0, runs1, rstride, sg->runn, t);
+            nw = use_bits ? !bit_test(Ub, x - c.bit_base) : !in_runs(x, E0, n0, runs1, rstride, sg->runn, t);
           }
           const unsigned bal = __ballot_sync(gmask, nw) >> gsrc;
           if (nw) Rp[rn + __popc(bal & ((1u << gl) - 1u))] = make_int2(x, 0);
@@ -407,6 +484,12 @@ __device__ __forceinline__ void motif_run_task(const MotifCtx& c, unsigned long 
         }
         const int m = (nE - startE) + rn;
         __syncwarp(gmask);
+        if (use_bits) {
+          bits_flip_list<W>(Ub, c.bit_base, Rp, rn, true, gl);
+          if (p == K - 3) bits_flip_list<W>(Eb, c.bit_base, Ep, m, true, gl);
+          bdepth = p;
+          __syncwarp(gmask);
+        }
         if (p < level) {
           // replaying a donated prefix: the path fixes the member expanded at level p
           const int idx = (p < QPATH) ? path[p] : -1;
@@ -471,7 +554,12 @@ __device__ __forceinline__ void motif_run_task(const MotifCtx& c, unsigned long 
       }
       if (!found) break;
     }
+    if (use_bits) drop_levels(1);
     if (bad) break;
+  }
+  if (use_bits) {
+    bits_flip_ids<W>(Ub, c.bit_base, E0, n0, false, gl);
+    if (K == 3) bits_flip_ids<W>(Eb, c.bit_base, E0, n0, false, gl);
   }
   __syncwarp();
   if (c.per_root) {
