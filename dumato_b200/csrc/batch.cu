@@ -42,6 +42,10 @@ struct BatchQuery {
   int bit_words;        // motifs: membership bitmap words (0 = none)
   const int32_t* q2c;   // motifs: quick code -> class
   unsigned long long* out;  // count (cliques) or class counters (motifs)
+  // the task contexts of this query, built on the host: the kernel passes references into
+  // this table, so no per-task copy of the load-balancer arguments lands in local memory
+  CliqueArgs cargs;
+  MotifCtx mctx;
 };
 
 struct BatchArgs {
@@ -86,40 +90,17 @@ __device__ __forceinline__ int batch_find_query(const int32_t* vbase, int n, int
 template <int K, int M>
 __device__ unsigned long long batch_clique(const BatchArgs& a, const BatchQuery& q, unsigned char* wsm,
                                            int32_t* arena, int root, int b, int e) {
-  CliqueArgs ca;
-  ca.g = a.g;
-  ca.roots = nullptr;
-  ca.n_roots = 0;
-  ca.lb = a.lb;
-  ca.lb.hungry_trigger = q.trigger;
-  ca.lb.min_split = 32;
-  ca.parts = nullptr;
-  ca.arena = arena;
-  ca.arena_dcap = q.arena_dcap;
-  ca.list_threshold = q.list_threshold;
-  ca.per_root = nullptr;
-  return clique_task<K, M>(ca, wsm, root, b, e, arena);
+  return clique_task<K, M>(q.cargs, wsm, root, b, e, arena);
 }
 
 template <int K, int W>
 __device__ void batch_motif(const BatchArgs& a, const BatchQuery& q, unsigned char* wsm, int2* arena,
                             uint32_t* bits, int v0, int b, int e, int level, const int* path,
                             unsigned long long& nodes) {
-  MotifCtx c;
-  c.g = a.g;
-  c.lb = a.lb;
-  c.lb.hungry_trigger = q.trigger;
-  c.lb.min_split = 4;
-  c.q2c = q.q2c;
-  c.maxdeg = q.maxdeg;
-  c.arena_stride = q.arena_stride;
-  c.per_root = nullptr;
-  c.bit_base = q.vbase;
-  c.bit_words = bits ? q.bit_words : 0;
   MotifShared* ws = reinterpret_cast<MotifShared*>(wsm);
   MotifGroup* groups = reinterpret_cast<MotifGroup*>(ws + 1);
   unsigned long long tn = 0;
-  motif_run_task<K, W>(c, q.out, ws, groups, arena, bits, v0, b, e, level, path, tn);
+  motif_run_task<K, W>(q.mctx, q.out, ws, groups, arena, bits, v0, b, e, level, path, tn);
   // every lane of a group counted the group's nodes: keep the leaders' counts
   if ((lane_id() & (W - 1)) == 0) nodes += tn;
 }
@@ -141,7 +122,7 @@ __global__ void batch_reset(DevCounters* c, int n_roots) {
 }
 
 template <int M>
-__global__ void __launch_bounds__(32 * BATCH_WARPS, 4) batch_kernel(BatchArgs a) {
+__global__ void __launch_bounds__(32 * BATCH_WARPS, 4) batch_kernel(const __grid_constant__ BatchArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int lane = lane_id();
   const int wib = warp_in_block();
@@ -592,10 +573,6 @@ int dm_batch_create(const dm_query* queries, int32_t n, const dm_opts* opts, int
     if (ce != cudaSuccess)
       return fail_release(b, fail(DM_ECUDA, std::string("dm_batch_create: bitmaps: ") + cudaGetErrorString(ce)));
   }
-  if ((rc = upload(reinterpret_cast<void**>(&b->d_desc), desc.data(), sizeof(BatchQuery) * desc.size())))
-    return fail_release(b, rc);
-  DM_CUDA(cudaStreamSynchronize(b->stream));
-
   BatchArgs& a = b->args;
   a.g = GraphView{b->d_row, b->d_deg, b->d_adj, (int32_t)total_v};
   a.roots = b->d_roots;
@@ -604,13 +581,40 @@ int dm_batch_create(const dm_query* queries, int32_t n, const dm_opts* opts, int
                 reinterpret_cast<QSlot*>(reinterpret_cast<char*>(b->d_queue) + sizeof(QHeader) * QUEUE_SHARDS),
                 QUEUE_SHARD_SLOTS, 0, ctx.donations_per_warp, (long long)ctx.donate_after_us * 1000ll,
                 (long long)ctx.timeout_ms * 1000000ll, ctx.test_stall, 32, QUEUE_SHARDS};
-  a.queries = b->d_desc;
   a.vbase = b->d_vbase;
   a.n_queries = n;
   a.arena = b->d_arena;
   a.arena_bytes = arena_bytes;
   a.bits = b->d_bits;
   a.bits_words = bits_words;
+  // per-query task contexts (the query's donation trigger and split granularity)
+  for (int32_t i = 0; i < n; ++i) {
+    BatchQuery& d = desc[i];
+    std::memset(&d.cargs, 0, sizeof(d.cargs));
+    std::memset(&d.mctx, 0, sizeof(d.mctx));
+    if (d.kind == DM_QUERY_CLIQUE) {
+      d.cargs.g = a.g;
+      d.cargs.lb = a.lb;
+      d.cargs.lb.hungry_trigger = d.trigger;
+      d.cargs.lb.min_split = 32;
+      d.cargs.arena_dcap = d.arena_dcap;
+      d.cargs.list_threshold = d.list_threshold;
+    } else {
+      d.mctx.g = a.g;
+      d.mctx.lb = a.lb;
+      d.mctx.lb.hungry_trigger = d.trigger;
+      d.mctx.lb.min_split = 4;
+      d.mctx.q2c = d.q2c;
+      d.mctx.maxdeg = d.maxdeg;
+      d.mctx.arena_stride = d.arena_stride;
+      d.mctx.bit_base = d.vbase;
+      d.mctx.bit_words = b->d_bits ? d.bit_words : 0;
+    }
+  }
+  if ((rc = upload(reinterpret_cast<void**>(&b->d_desc), desc.data(), sizeof(BatchQuery) * desc.size())))
+    return fail_release(b, rc);
+  a.queries = b->d_desc;
+  DM_CUDA(cudaStreamSynchronize(b->stream));
 
   // ---- capture: reset, clear, launch, read back ----
   ce = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);

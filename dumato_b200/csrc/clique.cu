@@ -10,7 +10,7 @@
 namespace dmb {
 
 template <int K, int M>
-__global__ void __launch_bounds__(256) clique_kernel(CliqueArgs a) {
+__global__ void __launch_bounds__(256) clique_kernel(const __grid_constant__ CliqueArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
   constexpr WarpLayout LY = warp_layout(M);
   const int lane = lane_id();

@@ -24,7 +24,7 @@ struct MotifArgs {
 };
 
 template <int K, int W>
-__global__ void __launch_bounds__(32 * MOTIF_WARPS, 4) motif_kernel(MotifArgs a) {
+__global__ void __launch_bounds__(32 * MOTIF_WARPS, 4) motif_kernel(const __grid_constant__ MotifArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
   unsigned long long* bhist = reinterpret_cast<unsigned long long*>(smem);
   unsigned char* wbase = smem + sizeof(unsigned long long) * ((a.n_classes + 1) & ~1);

@@ -158,12 +158,12 @@ __device__ __forceinline__ void mask_hist(const int2* list, int lo, int hi, unsi
   __syncwarp(gmask);
 }
 
-// Flushes the group's leaf-mask histogram into the class counters.
-template <int W>
+// Flushes the group's leaf-mask histogram (masks below NMASK) into the class counters.
+template <int W, int NMASK>
 __device__ __forceinline__ void flush_masks(MotifGroup* sg, const int32_t* q2c, unsigned quick_p, int off,
                                             unsigned long long* hist, unsigned long long& task_cnt, int gl,
                                             unsigned gmask) {
-  for (int m = gl; m < 64; m += W) {
+  for (int m = gl; m < NMASK; m += W) {
     const unsigned c = sg->mh[m];
     if (c) {
       sg->mh[m] = 0;
@@ -243,7 +243,9 @@ __device__ __forceinline__ void motif_run_task(const MotifCtx& c, unsigned long 
   int2* const runs1 = ext_at(K - 2);
   const size_t rstride = md + 32;
   auto run_at = [&](int t) -> int2* { return runs1 + (size_t)(t - 1) * rstride; };
-  const bool use_bits = warp_bits != nullptr && c.bit_words > 0;
+  // (k = 3 has a single level: setting and clearing E_0's bits per task costs more than the
+  // binary searches it saves)
+  const bool use_bits = K >= 4 && warp_bits != nullptr && c.bit_words > 0;
   uint32_t* const Ub = use_bits ? warp_bits + (size_t)gi * 2 * c.bit_words : nullptr;
   uint32_t* const Eb = use_bits ? Ub + c.bit_words : nullptr;
   int bdepth = 0;  // levels 1..bdepth have their run (and, at level k-3, E) bits set
@@ -369,7 +371,7 @@ __device__ __forceinline__ void motif_run_task(const MotifCtx& c, unsigned long 
           for (int o = W / 2; o > 0; o >>= 1) ex += __shfl_xor_sync(gmask, ex, o);
           if (gl == 0 && ex) atomicAdd(&sg->mh[1 << p], ex);
           __syncwarp(gmask);
-          flush_masks<W>(sg, c.q2c, quick_p, leaf_off, hist, task_cnt, gl, gmask);
+          flush_masks<W, (1 << (K - 1))>(sg, c.q2c, quick_p, leaf_off, hist, task_cnt, gl, gmask);
         } else {
         const int gt = lower_bound(Nw, 0, dw, w + 1);
         const int dgt = dw - gt;
@@ -440,7 +442,7 @@ __device__ __forceinline__ void motif_run_task(const MotifCtx& c, unsigned long 
           if (ex) atomicAdd(&sg->mh[1 << p], ex);
         }
         __syncwarp(gmask);
-        flush_masks<W>(sg, c.q2c, quick_p, leaf_off, hist, task_cnt, gl, gmask);
+        flush_masks<W, (1 << (K - 1))>(sg, c.q2c, quick_p, leaf_off, hist, task_cnt, gl, gmask);
         }
       } else {
         // materialise E_{p} = inherited + excl(w), merged by vertex id; excl(w) is also run
