@@ -339,11 +339,12 @@ __device__ __forceinline__ void motif_run_task(const MotifCtx& c, unsigned long 
         // leaves: histogram the masks of E_{p} without writing it
         const int leaf_off = quick_off(K - 1);
         const int n_inh = nE - startE;
-        const int sw0 = lower_bound(Nw, 0, dw, v0 + 1);
-        const int above = dw - sw0;
+        // a short row is scanned whole (members up to v0 skipped) instead of searched for v0
+        const bool short_row = dw <= 2 * W;
+        const int sw0b = short_row ? 0 : lower_bound(Nw, 0, dw, v0 + 1);
         int usize = n0;
         for (int i = 1; i <= t; ++i) usize += sg->runn[i];
-        if (use_bits && above <= 4 * (n_inh + usize) + 128) {
+        if (use_bits && dw - sw0b <= 4 * (n_inh + usize) + 128) {
           // one pass over N(w) above v0: a neighbour outside U_t is a new member of E_{p}
           // (excl(w)); a neighbour in E_t above w is an inherited member adjacent to w; the
           // inherited members not adjacent to w come from the suffix's mask counts
@@ -357,8 +358,9 @@ __device__ __forceinline__ void motif_run_task(const MotifCtx& c, unsigned long 
           }
           __syncwarp(gmask);
           unsigned ex = 0;
-          for (int i = sw0 + gl; i < dw; i += W) {
+          for (int i = sw0b + gl; i < dw; i += W) {
             const int32_t x = Nw[i];
+            if (x <= v0) continue;
             const int xb = x - c.bit_base;
             if (!bit_test(Ub, xb)) {
               ++ex;
@@ -373,6 +375,8 @@ __device__ __forceinline__ void motif_run_task(const MotifCtx& c, unsigned long 
           __syncwarp(gmask);
           flush_masks<W, (1 << (K - 1))>(sg, c.q2c, quick_p, leaf_off, hist, task_cnt, gl, gmask);
         } else {
+        const int sw0 = short_row ? lower_bound(Nw, 0, dw, v0 + 1) : sw0b;
+        const int above = dw - sw0;
         const int gt = lower_bound(Nw, 0, dw, w + 1);
         const int dgt = dw - gt;
         // probe each inherited member in N(w), or take the suffix's mask counts and move
