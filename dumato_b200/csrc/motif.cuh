@@ -455,13 +455,13 @@ __device__ __forceinline__ void motif_run_task(const MotifCtx& c, unsigned long 
         int2* Ep = ext_at(p);
         int2* Rp = run_at(p);
         if (use_bits) drop_levels(p);  // the previous member's sets at levels >= p
-        const int sw0 = lower_bound(Nw, 0, dw, v0 + 1);
+        const int sw0 = dw <= 2 * W ? 0 : lower_bound(Nw, 0, dw, v0 + 1);
         int rn = 0;
         for (int i0 = sw0; i0 < dw; i0 += W) {
           const int i = i0 + gl;
           int32_t x = 0;
           bool nw = false;
-          if (i < dw) {
+          if (i < dw && Nw[i] > v0) {
             x = Nw[i];
             nw = use_bits ? !bit_test(Ub, x - c.bit_base) : !in_runs(x, E0, n0, runs1, rstride, sg->runn, t);
           }
