@@ -62,6 +62,9 @@ struct dm_graph {
   int32_t max_out_degree = 0;
   // k-independent predictor features per vertex (6 per vertex), for cliques and motifs
   std::vector<float> feat[2];
+  // padded device layout of the CSRs (0: undirected, 1: degree-ordered DAG), built on the
+  // first upload and kept, so uploading the graph again is a plain copy
+  std::vector<int32_t> pad_row[2], pad_deg[2], pad_adj[2];
   // device copies
   std::mutex mu;
   std::vector<dmb::DeviceGraph*> dev;

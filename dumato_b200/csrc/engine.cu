@@ -187,20 +187,29 @@ static DeviceSlot* slot_for(dm_graph* g, int dev) {
   return s;
 }
 
-// Pads rows to multiples of 4 ints (16 bytes) filled with INT32_MAX.
-static int upload_csr(const std::vector<int64_t>& row, const std::vector<int32_t>& adj, int32_t n, int32_t** d_row,
-                      int32_t** d_deg, int32_t** d_adj, cudaStream_t st) {
-  std::vector<int32_t> prow(n), pdeg(n);
-  int64_t total = 0;
-  for (int32_t v = 0; v < n; ++v) {
-    int64_t d = row[v + 1] - row[v];
-    prow[v] = (int32_t)total;
-    pdeg[v] = (int32_t)d;
-    total += (d + 3) & ~3ll;
-    if (total >= INT32_MAX) return fail(DM_EOVERFLOW, "padded adjacency exceeds 32-bit offsets");
+// Pads rows to multiples of 4 ints (16 bytes) filled with INT32_MAX; the padded layout is
+// built on the first upload of a graph and kept with it.
+static int upload_csr(const std::vector<int64_t>& row, const std::vector<int32_t>& adj, int32_t n,
+                      std::vector<int32_t>& prow, std::vector<int32_t>& pdeg, std::vector<int32_t>& padj,
+                      int32_t** d_row, int32_t** d_deg, int32_t** d_adj, cudaStream_t st) {
+  if (padj.empty()) {
+    prow.assign(n, 0);
+    pdeg.assign(n, 0);
+    int64_t total = 0;
+    for (int32_t v = 0; v < n; ++v) {
+      int64_t d = row[v + 1] - row[v];
+      prow[v] = (int32_t)total;
+      pdeg[v] = (int32_t)d;
+      total += (d + 3) & ~3ll;
+      if (total >= INT32_MAX) {
+        prow.clear();
+        pdeg.clear();
+        return fail(DM_EOVERFLOW, "padded adjacency exceeds 32-bit offsets");
+      }
+    }
+    padj.assign((size_t)std::max<int64_t>(total, 4), INT32_MAX);
+    for (int32_t v = 0; v < n; ++v) std::memcpy(padj.data() + prow[v], adj.data() + row[v], sizeof(int32_t) * pdeg[v]);
   }
-  std::vector<int32_t> padj((size_t)std::max<int64_t>(total, 4), INT32_MAX);
-  for (int32_t v = 0; v < n; ++v) std::memcpy(padj.data() + prow[v], adj.data() + row[v], sizeof(int32_t) * pdeg[v]);
   DM_CUDA(cudaMalloc(d_row, sizeof(int32_t) * std::max(n, 1)));
   DM_CUDA(cudaMalloc(d_deg, sizeof(int32_t) * std::max(n, 1)));
   DM_CUDA(cudaMalloc(d_adj, sizeof(int32_t) * padj.size()));
@@ -472,7 +481,8 @@ int dm_count_cliques(dm_graph* g, int32_t k, const dm_opts* o, uint64_t* count, 
   if ((rc = prepare_ws(ws, ctx.stream))) return rc;
   DM_CUDA(cudaEventRecord(ws.ev0, ctx.stream));
   if (!s->dg.has_oriented) {
-    rc = upload_csr(g->orow, g->oadj, g->n, &s->dg.d_orow, &s->dg.d_odeg, &s->dg.d_oadj, ctx.stream);
+    rc = upload_csr(g->orow, g->oadj, g->n, g->pad_row[1], g->pad_deg[1], g->pad_adj[1], &s->dg.d_orow,
+                    &s->dg.d_odeg, &s->dg.d_oadj, ctx.stream);
     if (rc) return rc;
     s->dg.has_oriented = true;
   }
@@ -618,7 +628,8 @@ int dm_count_motifs(dm_graph* g, int32_t k, const dm_dictionary* dict, const dm_
   if ((rc = prepare_ws(ws, ctx.stream))) return rc;
   DM_CUDA(cudaEventRecord(ws.ev0, ctx.stream));
   if (!s->dg.has_undirected) {
-    rc = upload_csr(g->row, g->adj, g->n, &s->dg.d_row, &s->dg.d_deg, &s->dg.d_adj, ctx.stream);
+    rc = upload_csr(g->row, g->adj, g->n, g->pad_row[0], g->pad_deg[0], g->pad_adj[0], &s->dg.d_row,
+                    &s->dg.d_deg, &s->dg.d_adj, ctx.stream);
     if (rc) return rc;
     s->dg.has_undirected = true;
   }
