@@ -29,7 +29,7 @@ LIB_PATH = _PKG / "libdmb200.so"
 DM_OK = 0
 STATUS_NAMES = {
     -1: "DM_EINVAL", -2: "DM_EIO", -3: "DM_EFORMAT", -4: "DM_ENOMEM", -5: "DM_ENODEVICE",
-    -6: "DM_ECUDA", -7: "DM_ETIMEOUT", -8: "DM_EOVERFLOW",
+    -6: "DM_ECUDA", -7: "DM_ETIMEOUT", -8: "DM_EOVERFLOW", -9: "DM_EINTERNAL",
 }
 
 GEN_ER, GEN_CHUNG_LU, GEN_RMAT = 0, 1, 2

@@ -658,7 +658,7 @@ int dm_batch_run(dm_batch* b, uint64_t* results, int64_t n_results, dm_stats* st
     queue_init_launch(b->d_queue, QUEUE_SHARDS, QUEUE_SHARD_SLOTS, b->stream);
     if (b->d_bits) cudaMemsetAsync(b->d_bits, 0, b->bits_bytes, b->stream);
     cudaStreamSynchronize(b->stream);
-    return fail(h.err == ERR_TIMEOUT ? DM_ETIMEOUT : DM_EOVERFLOW, "batch kernel reported error " + std::to_string(h.err));
+    return fail(kernel_status(h.err), "batch kernel reported error " + std::to_string(h.err));
   }
   if (b->n_results) std::memcpy(results, b->h_out, sizeof(uint64_t) * (size_t)b->n_results);
   if (st) {

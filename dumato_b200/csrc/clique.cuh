@@ -70,6 +70,35 @@ __device__ __forceinline__ unsigned long long count_rec(const Bits<NW>& S, const
   }
 }
 
+// count_rec at the top of a long item, reporting progress to the load balancer's watched
+// word every 16 subtrees: waiting warps treat a word that stops changing for the timeout as
+// a lost wake-up, so an item that runs for seconds on one lane must keep it moving.
+template <int D, int NW>
+__device__ __forceinline__ unsigned long long count_rec_hb(const Bits<NW>& S, const uint64_t* __restrict__ rows,
+                                                           unsigned long long* progress) {
+  if constexpr (D < 3) {
+    return count_rec<D, NW>(S, rows);
+  } else {
+    unsigned long long sum = 0;
+    unsigned sub = 0;
+#pragma unroll
+    for (int wi = 0; wi < NW; ++wi) {
+      uint64_t bits = S.w[wi];
+      while (bits) {
+        const int b = __ffsll((long long)bits) - 1;
+        bits &= bits - 1;
+        const uint64_t* rc = rows + (wi * 64 + b) * NW;
+        Bits<NW> T;
+#pragma unroll
+        for (int j = 0; j < NW; ++j) T.w[j] = (j < wi ? 0ull : (j == wi ? bits : S.w[j])) & rc[j];
+        if (popc(T) >= D) sum += count_rec<D - 1, NW>(T, rows);
+        if ((++sub & 15) == 0) atomicAdd(progress, 1ull);
+      }
+    }
+    return sum;
+  }
+}
+
 // Position of the j-th (0-based) set bit of an NW-word row.
 template <int NW>
 __device__ __forceinline__ int select_bit(const uint64_t* row, int j) {
@@ -200,7 +229,7 @@ constexpr int HEAVY_SLOTS = 32;
 // (returns without counting) when a heavy slot is free.
 template <int K, int NW>
 __device__ __forceinline__ unsigned long long bitmap_item(int it, const uint64_t* rows, const int32_t* sE, int d,
-                                                          int* hn, int* heavy) {
+                                                          int* hn, int* heavy, unsigned long long* progress) {
   if constexpr (K == 3) {
     Bits<NW> S;
 #pragma unroll
@@ -226,7 +255,7 @@ __device__ __forceinline__ unsigned long long bitmap_item(int it, const uint64_t
           }
         }
       }
-      return count_rec<(K >= 5 ? K - 4 : 0), NW>(S, rows);
+      return count_rec_hb<(K >= 5 ? K - 4 : 0), NW>(S, rows, progress);
     }
   }
 }
@@ -234,7 +263,8 @@ __device__ __forceinline__ unsigned long long bitmap_item(int it, const uint64_t
 // Warp-cooperative run of one heavy item: the third local vertex c3 is spread over the
 // lanes (the j-th member of the candidate set goes to lane j mod 32).
 template <int K, int NW>
-__device__ __forceinline__ unsigned long long heavy_item(int it, const uint64_t* rows, const int32_t* sE, int d) {
+__device__ __forceinline__ unsigned long long heavy_item(int it, const uint64_t* rows, const int32_t* sE, int d,
+                                                         unsigned long long* progress) {
   const int lane = lane_id();
   const int c1 = lower_bound(sE, 0, d + 1, it + 1) - 1;
   const int c2 = select_bit<NW>(rows + c1 * NW, it - sE[c1]);
@@ -254,7 +284,7 @@ __device__ __forceinline__ unsigned long long heavy_item(int it, const uint64_t*
       Bits<NW> T;
 #pragma unroll
       for (int w = 0; w < NW; ++w) T.w[w] = (w < wi ? 0ull : (w == wi ? bits : S.w[w])) & rc[w];
-      if (popc(T) >= K - 4) sum += count_rec<(K >= 6 ? K - 5 : 0), NW>(T, rows);
+      if (popc(T) >= K - 4) sum += count_rec_hb<(K >= 6 ? K - 5 : 0), NW>(T, rows, progress);
     }
   }
   return sum;
@@ -321,11 +351,11 @@ __device__ unsigned long long bitmap_task(const CliqueArgs& a, unsigned char* ws
   while (true) {
     const int it = range_take(range);
     if (it < 0) break;
-    cnt += bitmap_item<K, NW>(it, rows, sE, d, hn, heavy);
+    cnt += bitmap_item<K, NW>(it, rows, sE, d, hn, heavy, &a.lb.ctr->progress);
     if ((++done & 15) == 0) {
       int ob = 0, oe = 0;
       if (range_maybe_donate(a.lb, range, root, donations_left, t_start, busy, ob, oe)) {
-        for (int j = ob; j < oe; ++j) cnt += bitmap_item<K, NW>(j, rows, sE, d, nullptr, nullptr);
+        for (int j = ob; j < oe; ++j) cnt += bitmap_item<K, NW>(j, rows, sE, d, nullptr, nullptr, &a.lb.ctr->progress);
       }
       if ((done & 255) == 0) atomicAdd(&a.lb.ctr->progress, 256ull);
     }
@@ -334,7 +364,7 @@ __device__ unsigned long long bitmap_task(const CliqueArgs& a, unsigned char* ws
   if constexpr (K >= 6) {
     const int nh = min(*hn, HEAVY_SLOTS);
     for (int h = 0; h < nh; ++h) {
-      cnt += heavy_item<K, NW>(heavy[h], rows, sE, d);
+      cnt += heavy_item<K, NW>(heavy[h], rows, sE, d, &a.lb.ctr->progress);
       if (lane == 0) atomicAdd(&a.lb.ctr->progress, 1ull);
     }
     __syncwarp();

@@ -210,15 +210,26 @@ static int upload_csr(const std::vector<int64_t>& row, const std::vector<int32_t
     padj.assign((size_t)std::max<int64_t>(total, 4), INT32_MAX);
     for (int32_t v = 0; v < n; ++v) std::memcpy(padj.data() + prow[v], adj.data() + row[v], sizeof(int32_t) * pdeg[v]);
   }
-  DM_CUDA(cudaMalloc(d_row, sizeof(int32_t) * std::max(n, 1)));
-  DM_CUDA(cudaMalloc(d_deg, sizeof(int32_t) * std::max(n, 1)));
-  DM_CUDA(cudaMalloc(d_adj, sizeof(int32_t) * padj.size()));
-  if (n) {
-    DM_CUDA(cudaMemcpyAsync(*d_row, prow.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, st));
-    DM_CUDA(cudaMemcpyAsync(*d_deg, pdeg.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, st));
+  // the three buffers are published together: a failure frees what was allocated
+  int32_t *r = nullptr, *d = nullptr, *a = nullptr;
+  cudaError_t e = cudaMalloc(&r, sizeof(int32_t) * std::max(n, 1));
+  if (e == cudaSuccess) e = cudaMalloc(&d, sizeof(int32_t) * std::max(n, 1));
+  if (e == cudaSuccess) e = cudaMalloc(&a, sizeof(int32_t) * padj.size());
+  if (e == cudaSuccess && n) e = cudaMemcpyAsync(r, prow.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess && n) e = cudaMemcpyAsync(d, pdeg.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(a, padj.data(), sizeof(int32_t) * padj.size(), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) {
+    cudaFree(r);
+    cudaFree(d);
+    cudaFree(a);
+    return fail(e == cudaErrorMemoryAllocation ? DM_ENOMEM : DM_ECUDA,
+                std::string("graph upload failed: ") + cudaGetErrorString(e));
   }
-  DM_CUDA(cudaMemcpyAsync(*d_adj, padj.data(), sizeof(int32_t) * padj.size(), cudaMemcpyHostToDevice, st));
-  DM_CUDA(cudaStreamSynchronize(st));
+  *d_row = r;
+  *d_deg = d;
+  *d_adj = a;
   return DM_OK;
 }
 
@@ -584,7 +595,7 @@ int dm_count_cliques(dm_graph* g, int32_t k, const dm_opts* o, uint64_t* count, 
   cudaEventElapsedTime(&kms, ws.k0, ws.k1);
   cudaEventElapsedTime(&pms, ws.ev0, ws.k0);
   if (h.err)
-    return fail(h.err == ERR_TIMEOUT ? DM_ETIMEOUT : DM_EOVERFLOW,
+    return fail(kernel_status(h.err),
                 "clique kernel reported error " + std::to_string(h.err));
   *count = h.count;
   if (want_log)
@@ -768,7 +779,7 @@ int dm_count_motifs(dm_graph* g, int32_t k, const dm_dictionary* dict, const dm_
   cudaEventElapsedTime(&kms, ws.k0, ws.k1);
   cudaEventElapsedTime(&pms, ws.ev0, ws.k0);
   if (h.err)
-    return fail(h.err == ERR_TIMEOUT ? DM_ETIMEOUT : DM_EOVERFLOW,
+    return fail(kernel_status(h.err),
                 "motif kernel reported error " + std::to_string(h.err));
   if (st) {
     std::memset(st, 0, sizeof(*st));

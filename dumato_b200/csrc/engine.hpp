@@ -42,6 +42,13 @@ constexpr int ERR_ARENA_OVERFLOW = 1;
 constexpr int ERR_TIMEOUT = 2;
 constexpr int ERR_BAD_TASK = 3;
 
+// Status of a call whose kernel raised device error word `err` (non-zero): a bounded wait
+// that gave up is DM_ETIMEOUT, an exceeded capacity bound DM_EOVERFLOW, and a task the
+// kernel could not place (its own bookkeeping disagreeing with the graph) DM_EINTERNAL.
+inline int kernel_status(int err) {
+  return err == ERR_TIMEOUT ? DM_ETIMEOUT : (err == ERR_ARENA_OVERFLOW ? DM_EOVERFLOW : DM_EINTERNAL);
+}
+
 struct GraphView {
   const int32_t* row;   // padded row starts
   const int32_t* deg;

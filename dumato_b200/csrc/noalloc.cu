@@ -10,12 +10,16 @@
 // The array below is a file-scope __device__ variable: every GPU that loads the library
 // holds NOALLOC_SCRATCH_BYTES of it until the process exits. In host code its name is
 // only a host-side stand-in for the device object; handing that name to a kernel would
-// fault, or silently use the wrong memory where the GPU can reach host memory. The device
-// address is obtained once per device with cudaGetSymbolAddress (with that device current)
-// and that address is what the kernel receives.
+// fault, or silently use the wrong memory where the GPU can reach host memory. Every call
+// resolves the device address with cudaGetSymbolAddress (on the current device, in the
+// current context) and hands that address to the kernels; nothing about the array is
+// cached on the host. Whether the donation queue inside it is in its empty state is also
+// kept on the device, in a tag word that the set-up kernel checks at the start of every
+// call: a context that was reset or re-created loads the module again with the array
+// zeroed, so the tag is missing and the queue is rebuilt there.
 #include <cuda_runtime.h>
 
-#include <mutex>
+#include <algorithm>
 #include <string>
 
 #include "engine.hpp"
@@ -29,54 +33,68 @@ constexpr int NOALLOC_QUEUE_SLOTS = 4096;
 // path, which needs no per-warp arena.
 constexpr int NOALLOC_MAX_OUT_DEGREE = 256;
 constexpr size_t NOALLOC_COUNTERS_BYTES = (sizeof(DevCounters) + 255) / 256 * 256;
+constexpr size_t NOALLOC_TAG_BYTES = 256;
 constexpr size_t NOALLOC_SCRATCH_BYTES =
-    NOALLOC_COUNTERS_BYTES + sizeof(QHeader) + sizeof(QSlot) * (size_t)NOALLOC_QUEUE_SLOTS;
+    NOALLOC_COUNTERS_BYTES + NOALLOC_TAG_BYTES + sizeof(QHeader) + sizeof(QSlot) * (size_t)NOALLOC_QUEUE_SLOTS;
+// Tag word value meaning "the queue below is in its empty state".
+constexpr unsigned NOALLOC_QUEUE_READY = 0x51554555u;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH_BYTES];
 
-constexpr int NOALLOC_MAX_DEVICES = 64;
-static std::mutex g_noalloc_mu;
-static void* g_noalloc_ptr[NOALLOC_MAX_DEVICES];  // device address of the scratch, per device
+struct NoallocParts {
+  DevCounters* ctr;
+  unsigned* tag;
+  QHeader* qh;
+  QSlot* q;
+};
 
-__global__ void noalloc_queue_init(QHeader* h, QSlot* q, int cap) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i == 0) {
-    h->write_pos = 0;
-    h->read_pos = 0;
-  }
-  if (i < cap) {
-    q[i].seq = (unsigned)i;
-    q[i].root = q[i].begin = q[i].end = q[i].level = 0;
-  }
+static NoallocParts noalloc_parts(void* base) {
+  char* b = reinterpret_cast<char*>(base);
+  NoallocParts p;
+  p.ctr = reinterpret_cast<DevCounters*>(b);
+  p.tag = reinterpret_cast<unsigned*>(b + NOALLOC_COUNTERS_BYTES);
+  p.qh = reinterpret_cast<QHeader*>(b + NOALLOC_COUNTERS_BYTES + NOALLOC_TAG_BYTES);
+  p.q = reinterpret_cast<QSlot*>(b + NOALLOC_COUNTERS_BYTES + NOALLOC_TAG_BYTES + sizeof(QHeader));
+  return p;
 }
 
-// The counters start every call at zero, with every root pending.
-__global__ void noalloc_reset_counters(DevCounters* c, int n_roots) {
-  int* w = reinterpret_cast<int*>(c);
+// Start of every call (one block): zero the counters with every root pending, and put the
+// queue in its empty state unless the tag says it already is (the kernels leave it empty
+// after a call that raised no error; a call that raised one clears the tag).
+__global__ void __launch_bounds__(1024) noalloc_setup(NoallocParts p, int n_roots, int cap) {
+  __shared__ int rebuild;
+  if (threadIdx.x == 0) rebuild = *reinterpret_cast<volatile unsigned*>(p.tag) != NOALLOC_QUEUE_READY;
+  int* w = reinterpret_cast<int*>(p.ctr);
   for (int i = threadIdx.x; i < (int)(sizeof(DevCounters) / sizeof(int)); i += blockDim.x) w[i] = 0;
   __syncthreads();
-  if (threadIdx.x == 0) c->pending = n_roots;
+  if (rebuild) {
+    if (threadIdx.x == 0) {
+      p.qh->write_pos = 0;
+      p.qh->read_pos = 0;
+    }
+    for (int i = threadIdx.x; i < cap; i += blockDim.x) {
+      p.q[i].seq = (unsigned)i;
+      p.q[i].root = p.q[i].begin = p.q[i].end = p.q[i].level = 0;
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    p.ctr->pending = n_roots;
+    if (rebuild) *p.tag = NOALLOC_QUEUE_READY;
+  }
 }
 
-// Set-up, once per device with that device current: resolve the scratch's device address
-// and put its queue in the empty state.
-static int noalloc_scratch(int dev, cudaStream_t st, void** out) {
-  if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return fail(DM_EINVAL, "device ordinal out of range");
-  std::lock_guard<std::mutex> lk(g_noalloc_mu);
-  if (!g_noalloc_ptr[dev]) {
-    void* p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess || !p)
-      return fail(DM_ECUDA, std::string("cudaGetSymbolAddress of the fixed scratch failed: ") + cudaGetErrorString(e));
-    char* base = reinterpret_cast<char*>(p);
-    QHeader* h = reinterpret_cast<QHeader*>(base + NOALLOC_COUNTERS_BYTES);
-    QSlot* q = reinterpret_cast<QSlot*>(base + NOALLOC_COUNTERS_BYTES + sizeof(QHeader));
-    noalloc_queue_init<<<(NOALLOC_QUEUE_SLOTS + 255) / 256, 256, 0, st>>>(h, q, NOALLOC_QUEUE_SLOTS);
-    e = cudaGetLastError();
-    if (e != cudaSuccess) return fail(DM_ECUDA, std::string("scratch set-up failed: ") + cudaGetErrorString(e));
-    g_noalloc_ptr[dev] = p;
-  }
-  *out = g_noalloc_ptr[dev];
+// After a call whose kernel raised an error: donations may be left in the queue, so the
+// next call's set-up rebuilds it.
+__global__ void noalloc_invalidate(unsigned* tag) { *tag = 0u; }
+
+// Device address of the fixed scratch in the current context.
+static int noalloc_scratch(void** out) {
+  void* p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess || !p)
+    return fail(DM_ECUDA, std::string("cudaGetSymbolAddress of the fixed scratch failed: ") + cudaGetErrorString(e));
+  *out = p;
   return DM_OK;
 }
 
@@ -107,11 +125,10 @@ extern "C" int dm_count_cliques_noalloc(const int32_t* d_row, const int32_t* d_d
   ctx.stream = reinterpret_cast<cudaStream_t>(stream);
   DM_CUDA(cudaDeviceGetAttribute(&ctx.num_sms, cudaDevAttrMultiProcessorCount, dev));
   void* scratch = nullptr;
-  int rc = noalloc_scratch(dev, ctx.stream, &scratch);
+  int rc = noalloc_scratch(&scratch);
   if (rc) return rc;
-  char* base = reinterpret_cast<char*>(scratch);
-  DevCounters* ctr = reinterpret_cast<DevCounters*>(base);
-  noalloc_reset_counters<<<1, 128, 0, ctx.stream>>>(ctr, n_roots);
+  const NoallocParts parts = noalloc_parts(scratch);
+  noalloc_setup<<<1, 1024, 0, ctx.stream>>>(parts, n_roots, NOALLOC_QUEUE_SLOTS);
   DM_CUDA(cudaGetLastError());
   int grid = 0;
   if (n_roots > 0) {
@@ -120,9 +137,10 @@ extern "C" int dm_count_cliques_noalloc(const int32_t* d_row, const int32_t* d_d
     L.k = k;
     L.roots = d_roots;
     L.n_roots = n_roots;
-    L.ctr = ctr;
-    L.queue = base + NOALLOC_COUNTERS_BYTES;
+    L.ctr = parts.ctr;
+    L.queue = parts.qh;
     L.qcap = NOALLOC_QUEUE_SLOTS;
+    L.nq = 1;
     L.max_donations = ctx.donations_per_warp;
     L.nwmax = std::min(4, std::max(1, (max_out_degree + 63) / 64));
     L.list_threshold = 64 * L.nwmax;
@@ -130,15 +148,12 @@ extern "C" int dm_count_cliques_noalloc(const int32_t* d_row, const int32_t* d_d
     if (rc) return rc;
   }
   DevCounters h;
-  DM_CUDA(cudaMemcpyAsync(&h, ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost, ctx.stream));
+  DM_CUDA(cudaMemcpyAsync(&h, parts.ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost, ctx.stream));
   DM_CUDA(cudaStreamSynchronize(ctx.stream));
   if (h.err) {
-    // a failed call can leave donations queued: empty the queue for the next call
-    QHeader* qh = reinterpret_cast<QHeader*>(base + NOALLOC_COUNTERS_BYTES);
-    QSlot* q = reinterpret_cast<QSlot*>(base + NOALLOC_COUNTERS_BYTES + sizeof(QHeader));
-    noalloc_queue_init<<<(NOALLOC_QUEUE_SLOTS + 255) / 256, 256, 0, ctx.stream>>>(qh, q, NOALLOC_QUEUE_SLOTS);
+    noalloc_invalidate<<<1, 1, 0, ctx.stream>>>(parts.tag);
     cudaStreamSynchronize(ctx.stream);
-    return fail(h.err == ERR_TIMEOUT ? DM_ETIMEOUT : DM_EOVERFLOW,
+    return fail(kernel_status(h.err),
                 "clique kernel reported error " + std::to_string(h.err) +
                     (h.err == ERR_ARENA_OVERFLOW ? " (a root's out-degree exceeds max_out_degree)" : ""));
   }

@@ -50,6 +50,7 @@ extern "C" {
 #define DM_ECUDA (-6)      /* a CUDA call failed */
 #define DM_ETIMEOUT (-7)   /* a bounded device-side wait gave up (error word set by a kernel) */
 #define DM_EOVERFLOW (-8)  /* a device-side capacity bound was exceeded */
+#define DM_EINTERNAL (-9)  /* a kernel found its own state inconsistent (a library fault, not the input) */
 
 typedef struct dm_graph dm_graph;
 typedef struct dm_dictionary dm_dictionary;
@@ -237,10 +238,15 @@ DM_API int dm_clique_work_model(dm_graph* g, int32_t k, uint64_t* nodes, uint64_
    must be at most 256: larger roots need per-warp scratch this entry point does not hold
    (use dm_count_cliques). Output: *count (host). Runs on `stream` and waits for it.
    Scratch: one fixed device array of about 260 KB (counters + donation queue) that every
-   GPU loading the library keeps until exit. The first call on a device resolves its
-   address and initialises it, so make that first call before any stream capture. Calls
-   share the array: calls that overlap on the GPU (other streams, threads or processes
-   sharing the context) race and must be serialised by the caller. */
+   GPU loading the library keeps until exit. Every call looks up the array's device address
+   in the current context and starts with a small set-up kernel that zeroes the counters
+   and, when a tag word in the array says the queue is not in its empty state (the first
+   call in a context, or the call after one that failed), rebuilds the queue; the first
+   call in a context also loads the array, so make that first call before any stream
+   capture. Calls share the array and each leaves its contents behind: calls that overlap
+   on the GPU (other streams, threads or processes sharing the context) race and must be
+   serialised by the caller. A root whose out-degree exceeds max_out_degree makes the call
+   return DM_EOVERFLOW; the next call starts clean. */
 DM_API int dm_count_cliques_noalloc(const int32_t* d_row, const int32_t* d_deg, const int32_t* d_adj,
                                     int32_t n_vertices, const int32_t* d_roots, int32_t n_roots,
                                     int32_t max_out_degree, int32_t k, uint64_t stream, uint64_t* count);

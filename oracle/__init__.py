@@ -48,6 +48,7 @@ def lib() -> ctypes.CDLL:
             "oracle_motifs_roots": (ctypes.c_int, [_P, ctypes.c_int, _P, ctypes.c_int32, _P, _P, ctypes.c_int64,
                                                    ctypes.c_int]),
             "oracle_motifs_brute": (ctypes.c_int, [_P, ctypes.c_int, _P, ctypes.c_int32, _P]),
+            "oracle_graphlet4": (ctypes.c_int, [_P, _P, ctypes.c_int]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -150,3 +151,59 @@ def motifs_brute(g: OracleGraph, k: int, q2c: np.ndarray, n_classes: int) -> np.
     hist = np.zeros(n_classes, np.uint64)
     lib().oracle_motifs_brute(g.h, k, q.ctypes.data, n_classes, hist.ctypes.data)
     return hist
+
+
+GRAPHLET4_TYPES = ("path", "claw", "cycle", "paw", "diamond", "clique")
+
+
+def graphlet4(g: OracleGraph, threads: int = 0) -> dict:
+    """Connected induced 4-vertex subgraphs of the whole graph by type, from closed-form
+    subgraph counts (no enumeration): {"path", "claw", "cycle", "paw", "diamond", "clique"}."""
+    out = np.zeros(6, np.uint64)
+    lib().oracle_graphlet4(g.h, out.ctypes.data, threads)
+    return {t: int(c) for t, c in zip(GRAPHLET4_TYPES, out)}
+
+
+def quick_edges(q: int, k: int) -> list[tuple[int, int]]:
+    """Edges of the k-vertex pattern whose quick code is q: the edge (v0, v1) is implicit and
+    vertex p >= 2 owns bits [(p-2)(p+1)/2, +p), bit j meaning the edge (v_j, v_p)
+    (src/main/DuMatoGPU.cu:858,932)."""
+    edges = [(0, 1)]
+    for p in range(2, k):
+        base = (p - 2) * (p + 1) // 2
+        for j in range(p):
+            if (q >> (base + j)) & 1:
+                edges.append((j, p))
+    return edges
+
+
+def graphlet4_type(edges) -> Optional[str]:
+    """Type of a 4-vertex pattern given by its edges (None when it is disconnected)."""
+    deg = [0] * 4
+    for a, b in edges:
+        deg[a] += 1
+        deg[b] += 1
+    # connectivity by a small union-find
+    par = list(range(4))
+
+    def find(x):
+        while par[x] != x:
+            x = par[x]
+        return x
+
+    for a, b in edges:
+        par[find(a)] = find(b)
+    if len({find(x) for x in range(4)}) != 1:
+        return None
+    ds = tuple(sorted(deg))
+    return {(1, 1, 2, 2): "path", (1, 1, 1, 3): "claw", (2, 2, 2, 2): "cycle", (1, 2, 2, 3): "paw",
+            (2, 2, 3, 3): "diamond", (3, 3, 3, 3): "clique"}[ds]
+
+
+def class_types4(q2c: np.ndarray, n_classes: int) -> list:
+    """Graphlet type of every class of a k = 4 dictionary (None for disconnected classes)."""
+    types = [None] * n_classes
+    for q, c in enumerate(np.asarray(q2c)):
+        if 0 <= c < n_classes and types[c] is None:
+            types[c] = graphlet4_type(quick_edges(q, 4)) or "disconnected"
+    return [None if t == "disconnected" else t for t in types]

@@ -633,3 +633,133 @@ int oracle_motifs_roots(const og_graph *g, int K, const int32_t *q2c, int32_t n_
   }
   return overflow ? -1 : 0;
 }
+
+/* ---------------- closed-form 4-vertex graphlet counts (independent check) ----------------
+   Connected induced 4-vertex subgraphs of the whole graph by isomorphism type, computed
+   WITHOUT enumerating them, so that the motif engine's k = 4 histogram can be checked on
+   graphs whose 4-subgraph count is far beyond any enumerator (the checker's own parity
+   is pinned by the enumerating oracle on small graphs). Non-induced copies of each type:
+     star (claw)  S = sum_v C(d_v, 3)
+     path P4      P = sum_{uv in E} (d_u - 1)(d_v - 1) - 3T          (T triangles)
+     paw          W = sum_v t_v (d_v - 2)                           (t_v triangles at v)
+     4-cycle      C = number of 4-cycles, each counted once from its highest-ranked vertex
+                      and the vertex opposite it (wedge counting in degree order)
+     diamond      D = sum_{uv in E} C(t_uv, 2)                      (t_uv triangles on uv)
+     K4           Q = 4-cliques
+   and the induced counts follow by removing the copies each denser type holds:
+     K4 = Q, diamond = D - 6Q, C4 = C - diamond - 3Q, paw = W - 4 diamond - 12Q,
+     claw = S - paw - 2 diamond - 4Q, P4 = P - 2 paw - 4 C4 - 6 diamond - 12Q.
+   out[6] = {P4, claw, C4, paw, diamond, K4}. Self-loops are ignored. */
+int oracle_graphlet4(const og_graph *g, uint64_t *out, int threads) {
+  og_dag *d = make_dag(g);
+  const int32_t n = d->n;
+  int64_t *deg = (int64_t *)calloc((size_t)n + 1, sizeof(int64_t)); /* rank space */
+  for (int32_t r = 0; r < n; ++r) {
+    const int32_t v = d->orig[r];
+    int64_t x = 0;
+    for (int64_t e = g->off[v]; e < g->off[v + 1]; ++e) x += g->adj[e] != v;
+    deg[r] = x;
+  }
+  /* undirected rank-space adjacency: in-neighbours (lower rank) then out-neighbours */
+  int64_t *uoff = (int64_t *)calloc((size_t)n + 1, sizeof(int64_t));
+  for (int32_t r = 0; r < n; ++r) uoff[r + 1] = deg[r];
+  for (int32_t r = 0; r < n; ++r) uoff[r + 1] += uoff[r];
+  int32_t *uadj = (int32_t *)malloc(sizeof(int32_t) * (size_t)(uoff[n] + 1));
+  int64_t *fill = (int64_t *)malloc(sizeof(int64_t) * ((size_t)n + 1));
+  memcpy(fill, uoff, sizeof(int64_t) * (size_t)n);
+  for (int32_t r = 0; r < n; ++r)
+    for (int64_t e = d->off[r]; e < d->off[r + 1]; ++e) uadj[fill[d->adj[e]]++] = r; /* in, ascending r */
+  for (int32_t r = 0; r < n; ++r)
+    for (int64_t e = d->off[r]; e < d->off[r + 1]; ++e) uadj[fill[r]++] = d->adj[e]; /* out, ascending */
+  free(fill);
+  const int64_t m_dag = d->off[n];
+  uint64_t *te = (uint64_t *)calloc((size_t)m_dag + 1, sizeof(uint64_t)); /* per DAG edge */
+  uint64_t *tv = (uint64_t *)calloc((size_t)n + 1, sizeof(uint64_t));
+  uint64_t T = 0;
+  const int nt = resolve_threads(threads);
+#pragma omp parallel for schedule(dynamic, 64) reduction(+ : T) num_threads(nt)
+  for (int32_t r = 0; r < n; ++r) {
+    for (int64_t p1 = d->off[r]; p1 < d->off[r + 1]; ++p1) {
+      const int32_t v = d->adj[p1];
+      int64_t i = p1 + 1, j = d->off[v];
+      while (i < d->off[r + 1] && j < d->off[v + 1]) {
+        if (d->adj[i] < d->adj[j]) ++i;
+        else if (d->adj[i] > d->adj[j]) ++j;
+        else {
+          const int32_t w = d->adj[i];
+#pragma omp atomic
+          te[p1]++;
+#pragma omp atomic
+          te[i]++;
+#pragma omp atomic
+          te[j]++;
+#pragma omp atomic
+          tv[r]++;
+#pragma omp atomic
+          tv[v]++;
+#pragma omp atomic
+          tv[w]++;
+          ++T;
+          ++i;
+          ++j;
+        }
+      }
+    }
+  }
+  uint64_t S = 0, P = 0, W = 0, D = 0, C = 0;
+  for (int32_t r = 0; r < n; ++r) {
+    const uint64_t x = (uint64_t)deg[r];
+    if (x >= 3) S += x * (x - 1) * (x - 2) / 6;
+    if (x >= 2) W += tv[r] * (x - 2);
+    for (int64_t e = d->off[r]; e < d->off[r + 1]; ++e) {
+      const uint64_t y = (uint64_t)deg[d->adj[e]];
+      P += (x - 1) * (y - 1);
+      D += te[e] * (te[e] - (te[e] > 0)) / 2;
+    }
+  }
+  P -= 3 * T;
+#pragma omp parallel num_threads(nt) reduction(+ : C)
+  {
+    uint32_t *cnt = (uint32_t *)calloc((size_t)n + 1, sizeof(uint32_t));
+    int32_t *touched = (int32_t *)malloc(sizeof(int32_t) * ((size_t)n + 1));
+#pragma omp for schedule(dynamic, 64)
+    for (int32_t u = 0; u < n; ++u) {
+      int64_t nt_ = 0;
+      for (int64_t e = uoff[u]; e < uoff[u + 1]; ++e) {
+        const int32_t v = uadj[e];
+        if (v >= u) break; /* in-neighbours come first, ascending */
+        for (int64_t f = uoff[v]; f < uoff[v + 1]; ++f) {
+          const int32_t w = uadj[f];
+          if (w >= u) continue;
+          if (cnt[w]++ == 0) touched[nt_++] = w;
+        }
+      }
+      for (int64_t t = 0; t < nt_; ++t) {
+        const uint64_t c = cnt[touched[t]];
+        C += c * (c - (c > 0)) / 2;
+        cnt[touched[t]] = 0;
+      }
+    }
+    free(cnt);
+    free(touched);
+  }
+  free(uadj);
+  free(uoff);
+  free(te);
+  free(tv);
+  free(deg);
+  free_dag(d);
+  const uint64_t Q = oracle_clique_dag_bytes(g, 4, NULL, threads);
+  const uint64_t dia = D - 6 * Q;
+  const uint64_t c4 = C - dia - 3 * Q;
+  const uint64_t paw = W - 4 * dia - 12 * Q;
+  const uint64_t claw = S - paw - 2 * dia - 4 * Q;
+  const uint64_t p4 = P - 2 * paw - 4 * c4 - 6 * dia - 12 * Q;
+  out[0] = p4;
+  out[1] = claw;
+  out[2] = c4;
+  out[3] = paw;
+  out[4] = dia;
+  out[5] = Q;
+  return 0;
+}

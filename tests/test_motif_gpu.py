@@ -122,11 +122,14 @@ def test_matches_reference_binaries(dm, gpu, tmp_path):
     graphs = {"test": lambda: dm.Graph.load_edgelist(GOLDEN / "test.edgelist"),
               "citeseer": lambda: dm.Graph.load_edgelist(GOLDEN / "citeseer.edgelist"),
               "er2k_s1": lambda: workloads.make("er2k", 1),
-              "rmat2k_s3": lambda: dm.Graph.generate(dm.GEN_RMAT, 2000, 8000, seed=3)}
+              "rmat2k_s3": lambda: dm.Graph.generate(dm.GEN_RMAT, 2000, 8000, seed=3),
+              "chunglu18k_s1": lambda: workloads.make("chunglu18k", 1),
+              "rmat317k_s1": lambda: workloads.make("rmat317k", 1)}
     for name, entry in ref.items():
         g = graphs[name]()
-        for k, c in entry["clique"].items():
-            assert dm.count_cliques(g, int(k))[0] == c, (name, k)
+        for key in ("clique", "clique_lb_threshold30"):
+            for k, c in entry.get(key, {}).items():
+                assert dm.count_cliques(g, int(k))[0] == c, (name, key, k)
         for k, mot in entry["motifs"].items():
             k = int(k)
             z = np.load(GOLDEN / f"ref_dict_{k}.npz")

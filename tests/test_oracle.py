@@ -47,6 +47,30 @@ def test_per_root_sums_to_total(orc, dm):
     assert int(orc.clique_per_root(g, 4).sum()) == orc.clique_dfs(g, 4)
 
 
+LARGE_REF_GRAPHS = {"chunglu18k_s1": ("chunglu18k", 1), "rmat317k_s1": ("rmat317k", 1)}
+
+
+def _ref_motif_check(orc, g, k, mot, large):
+    """The reference's per-class counts (its own class ids) against the enumerating oracle,
+    or on graphs too large to enumerate on a CPU, against the closed forms (k = 3, 4)."""
+    rq2c = np.load(GOLDEN / f"ref_dict_{k}.npz")["quick_to_class"]
+    ncls = int(rq2c.max()) + 1
+    want = np.zeros(ncls, np.uint64)
+    for cls, cnt in mot["classes"].items():
+        want[int(cls)] = cnt
+    if not large:
+        return np.array_equal(orc.motifs(g, k, rq2c, ncls), want)
+    if k == 4:
+        types = orc.class_types4(rq2c, ncls)
+        got = {}
+        for c, t in enumerate(types):
+            if t is not None:
+                got[t] = got.get(t, 0) + int(want[c])
+        return got == orc.graphlet4(g)
+    tri, _ = orc.clique_dag_bytes(g, 3)
+    return sorted(int(x) for x in want if x) == sorted([tri, int(mot["total"]) - tri])
+
+
 def test_oracle_matches_reference_binaries(dm, orc):
     """Counts printed by the reference's own clique_PA / motifs_DM_WCLB on a B200
     (tests/golden/ref_counts.json, made by run_reference_binaries.py)."""
@@ -60,15 +84,58 @@ def test_oracle_matches_reference_binaries(dm, orc):
               "citeseer": lambda: orc.OracleGraph.load(GOLDEN / "citeseer.edgelist"),
               "er2k_s1": lambda: orc.OracleGraph.from_pairs(*workloads.make("er2k", 1).edges()),
               "rmat2k_s3": lambda: orc.OracleGraph.from_pairs(*dm.Graph.generate(dm.GEN_RMAT, 2000, 8000, seed=3).edges())}
+    for name, (w, seed) in LARGE_REF_GRAPHS.items():
+        graphs[name] = lambda w=w, seed=seed: orc.OracleGraph.from_pairs(*workloads.make(w, seed).edges())
     for name, entry in ref.items():
         g = graphs[name]()
-        for k, c in entry["clique"].items():
-            assert orc.clique_dfs(g, int(k)) == c, (name, k)
+        large = name in LARGE_REF_GRAPHS
+        for key in ("clique", "clique_lb_threshold30"):
+            for k, c in entry.get(key, {}).items():
+                got = orc.clique_dag_bytes(g, int(k))[0] if large else orc.clique_dfs(g, int(k))
+                assert got == c, (name, key, k)
         for k, mot in entry["motifs"].items():
-            k = int(k)
-            rq2c = np.load(GOLDEN / f"ref_dict_{k}.npz")["quick_to_class"]
-            h = orc.motifs(g, k, rq2c, int(rq2c.max()) + 1)
-            want = np.zeros_like(h)
-            for cls, cnt in mot["classes"].items():
-                want[int(cls)] = cnt
-            assert np.array_equal(h, want), (name, k)
+            assert _ref_motif_check(orc, g, int(k), mot, large), (name, k)
+
+
+def _by_type(orc, dm, og):
+    d = dm.Dictionary.generate(4)
+    q2c, _ = d.tables()
+    types = orc.class_types4(q2c, d.n_classes)
+    h = orc.motifs(og, 4, q2c, d.n_classes)
+    out = {t: 0 for t in orc.GRAPHLET4_TYPES}
+    for c, t in enumerate(types):
+        if t is not None:
+            out[t] += int(h[c])
+    return out
+
+
+@pytest.mark.parametrize("seed", range(4))
+def test_graphlet4_closed_form_matches_enumeration(dm, orc, seed):
+    """The closed-form 4-graphlet checker (used at full size, where no enumerator finishes)
+    agrees with the enumerating motif oracle on random graphs with self-loops and repeats."""
+    rng = np.random.default_rng(100 + seed)
+    n = int(rng.integers(20, 60))
+    m = int(rng.integers(n, 4 * n))
+    s, t = rng.integers(0, n, m), rng.integers(0, n, m)
+    og = orc.OracleGraph.from_pairs(s, t)
+    assert orc.graphlet4(og) == _by_type(orc, dm, og)
+
+
+@pytest.mark.parametrize("name", ["citeseer", "rmat2k"])
+def test_graphlet4_closed_form_on_skewed_graphs(dm, orc, name):
+    if name == "citeseer":
+        og = orc.OracleGraph.load(GOLDEN / "citeseer.edgelist")
+    else:
+        u, v = dm.Graph.generate(dm.GEN_RMAT, 2000, 8000, seed=3).edges()
+        og = orc.OracleGraph.from_pairs(u, v)
+    assert orc.graphlet4(og) == _by_type(orc, dm, og)
+
+
+def test_class_types_of_the_reference_dictionary(dm, orc):
+    """Every connected class of the k = 4 dictionary gets a distinct graphlet type."""
+    d = dm.Dictionary.generate(4)
+    q2c, _ = d.tables()
+    types = orc.class_types4(q2c, d.n_classes)
+    conn = d.connected()
+    assert sorted(t for t, c in zip(types, conn) if c) == sorted(orc.GRAPHLET4_TYPES)
+    assert all(t is None for t, c in zip(types, conn) if not c)
