@@ -52,10 +52,16 @@ def _stale(target: Path, deps: list[Path]) -> bool:
 
 
 def build(verbose: bool = False, ptxas_info: bool = False) -> Path:
+    headers = list(CSRC.glob("*.hpp")) + list(CSRC.glob("*.cuh")) + list((PKG.parent / "include").glob("*.h*"))
+    sources = [CSRC / s for s in LIB_SOURCES] + [CSRC / s for s in CLI_SOURCES.values()]
+    # a library and executables newer than every source need no object files (a copy of the
+    # tree that carries only the built outputs)
+    if not ptxas_info and not _stale(LIB, sources + headers) and \
+            all(not _stale(BIN / name, [LIB, CSRC / src] + headers) for name, src in CLI_SOURCES.items()):
+        return LIB
     BUILD.mkdir(exist_ok=True)
     BIN.mkdir(exist_ok=True)
     nvcc = _nvcc()
-    headers = list(CSRC.glob("*.hpp")) + list(CSRC.glob("*.cuh")) + [PKG.parent / "include" / "dumato_b200.h"]
     objs = []
     jobs = []
     for src in LIB_SOURCES:

@@ -17,8 +17,9 @@
 //       aggregate = popc at the last level.
 //   list path (larger d, or DM_MODE_LIST): the reference's list structure. Items are the
 //       first-level candidates c1; the warp extends sorted candidate lists level by level in
-//       a per-warp global arena by binary-search intersection and ballot compaction
-//       (DuMatoGPU.cu:317-328 write), counting the leaf level without writing it.
+//       a per-warp global arena with dm_gpm::extend_intersect (a merge of lane slices, or a
+//       probe of each candidate when the adjacency list is much longer) and counts the leaf
+//       level with dm_gpm::intersect_count without writing it.
 #pragma once
 
 #include <climits>
@@ -415,18 +416,12 @@ __device__ unsigned long long list_task(const CliqueArgs& a, unsigned char* wsm,
     const int32_t* B = a.g.adj + __ldg(a.g.row + c);
     const int nb = __ldg(a.g.deg + c);
     if constexpr (K == 3) {
-      unsigned s = 0;
-      for (int i = lane; i < na; i += 32) s += contains(B, nb, __ldg(A + i)) ? 1u : 0u;
-      cnt += s;
+      const int s = dm_gpm::intersect_count<32>(A, na, B, nb);
+      if (lane == 0) cnt += (unsigned)s;
     } else {
       // C1 = A cap N+(c), written to level 1 of the arena
       int32_t* out1 = my_arena + a.arena_dcap;
-      int m = 0;
-      for (int i0 = 0; i0 < na; i0 += 32) {
-        const int i = i0 + lane;
-        const int32_t x = i < na ? __ldg(A + i) : 0;
-        m += compact(out1, m, x, i < na && contains(B, nb, x));
-      }
+      const int m = dm_gpm::extend_intersect<32>(A, na, B, nb, out1);
       __syncwarp();
       if (lane == 0) {
         sPtr[1] = out1;
@@ -454,17 +449,11 @@ __device__ unsigned long long list_task(const CliqueArgs& a, unsigned char* wsm,
         const int32_t* B2 = a.g.adj + __ldg(a.g.row + v);
         const int nb2 = __ldg(a.g.deg + v);
         if (lvl + 1 == K - 2) {
-          unsigned s = 0;
-          for (int i = lane; i < na2; i += 32) s += contains(B2, nb2, A2[i]) ? 1u : 0u;
-          cnt += s;
+          const int s = dm_gpm::intersect_count<32>(A2, na2, B2, nb2);
+          if (lane == 0) cnt += (unsigned)s;
         } else {
           int32_t* out = my_arena + (size_t)(lvl + 1) * a.arena_dcap;
-          int m2 = 0;
-          for (int i0 = 0; i0 < na2; i0 += 32) {
-            const int i = i0 + lane;
-            const int32_t x = i < na2 ? A2[i] : 0;
-            m2 += compact(out, m2, x, i < na2 && contains(B2, nb2, x));
-          }
+          const int m2 = dm_gpm::extend_intersect<32>(A2, na2, B2, nb2, out);
           __syncwarp();
           ++lvl;
           if (lane == 0) {

@@ -9,6 +9,7 @@
 #include <string>
 
 #include "clique.cuh"
+#include "clique_cached.cuh"
 
 namespace dmb {
 
@@ -49,11 +50,8 @@ __global__ void __launch_bounds__(256) clique_kernel(const __grid_constant__ Cli
     }
     if (lane == 0) lb_done(a.lb, count);
   }
-  cnt = warp_sum_u64(cnt);
-  if (lane == 0) {
-    atomicAdd(&a.lb.ctr->count, cnt);
-    atomicAdd(&a.lb.ctr->tasks, ntasks);
-  }
+  dm_gpm::aggregate_counter<32>(&a.lb.ctr->count, cnt);
+  if (lane == 0) atomicAdd(&a.lb.ctr->tasks, ntasks);
 }
 
 // ---------------- host launcher ----------------
@@ -92,7 +90,43 @@ static int launch_nw(const CliqueArgs& a, int m, LaunchCtx& ctx, int* grid) {
   }
 }
 
+// Index-counting kernel: with query set, only the grid is computed.
+template <int K, int M, bool TMA>
+static int cached_k(CachedArgs* a, LaunchCtx& ctx, int* grid_out, bool query) {
+  const size_t smem = (size_t)cached_layout(M).total * (CLIQUE_BLOCK / 32);
+  auto kern = clique_cached_kernel<K, M, TMA>;
+  DM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int occ = 0;
+  DM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, CLIQUE_BLOCK, smem));
+  if (occ < 1) return fail(DM_EINVAL, "clique index kernel does not fit on an SM");
+  int grid = ctx.num_sms * occ;
+  if (ctx.threads > 0) grid = std::max(1, std::min(grid, (ctx.threads + CLIQUE_BLOCK - 1) / CLIQUE_BLOCK));
+  if (a->c.arena && grid * (CLIQUE_BLOCK / 32) > ctx.arena_warps)
+    grid = std::max(1, ctx.arena_warps / (CLIQUE_BLOCK / 32));
+  if (!query && grid != *grid_out) return fail(DM_EINVAL, "clique index kernel: grid differs from its plan");
+  *grid_out = grid;
+  if (query) return DM_OK;
+  const int warps = grid * (CLIQUE_BLOCK / 32);
+  a->c.lb.hungry_trigger = ctx.threshold >= 100 ? 0 : std::max(1, (ctx.threshold * warps + 99) / 100);
+  kern<<<grid, CLIQUE_BLOCK, smem, ctx.stream>>>(*a);
+  ctx.launches++;
+  DM_CUDA(cudaGetLastError());
+  return DM_OK;
+}
+
+template <int K>
+static int cached_nw(CachedArgs* a, int m, bool tma, LaunchCtx& ctx, int* grid, bool query) {
+  switch (m) {
+    case 1: return tma ? cached_k<K, 1, true>(a, ctx, grid, query) : cached_k<K, 1, false>(a, ctx, grid, query);
+    case 2: return tma ? cached_k<K, 2, true>(a, ctx, grid, query) : cached_k<K, 2, false>(a, ctx, grid, query);
+    case 3: return tma ? cached_k<K, 3, true>(a, ctx, grid, query) : cached_k<K, 3, false>(a, ctx, grid, query);
+    default: return tma ? cached_k<K, 4, true>(a, ctx, grid, query) : cached_k<K, 4, false>(a, ctx, grid, query);
+  }
+}
+
 // Launchers of the k ranges compiled in the other translation units.
+int clique_cached_k7_8(CachedArgs* a, int k, int m, bool tma, LaunchCtx& ctx, int* grid, bool query);
+
 int clique_launch_k7_8(const CliqueArgs& a, int k, int m, LaunchCtx& ctx, int* grid);
 int clique_launch_k9(const CliqueArgs& a, int m, LaunchCtx& ctx, int* grid);
 int clique_launch_k10(const CliqueArgs& a, int m, LaunchCtx& ctx, int* grid);

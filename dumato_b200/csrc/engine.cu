@@ -44,6 +44,19 @@ struct Workspace {
   size_t parts_cap = 0;
   uint32_t* d_bits = nullptr;       // motif membership bitmaps, all zero between calls
   size_t bits_cap = 0;
+  RootDesc* d_desc = nullptr;       // task list of a call on the clique index
+  size_t desc_cap = 0;
+  // learned schedule: MLP parameters, scratch and output task list
+  float* d_params = nullptr;
+  size_t params_cap = 0;
+  void* d_sched = nullptr;
+  size_t sched_cap = 0;
+  int32_t* d_sroots = nullptr;
+  size_t sroots_cap = 0;
+  int32_t* d_sparts = nullptr;
+  size_t sparts_cap = 0;
+  RootDesc* d_sdesc = nullptr;
+  size_t sdesc_cap = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, k0 = nullptr, k1 = nullptr;
 };
 
@@ -88,16 +101,18 @@ struct DeviceSlot {
   // motif roots (vertices with a neighbour above them) by descending upper degree
   int32_t* d_up_order = nullptr;
   int n_up = 0;
-  // last learned schedule per engine (0 = motifs, 1 = cliques), reused while its key holds
-  struct Learned {
-    bool valid = false;
-    int k = 0, world = 1, rank = 0;
-    uint64_t uid = 0, version = 0;
-    int32_t* d_roots = nullptr;
-    int32_t* d_parts = nullptr;
-    size_t cap = 0;
-    int n = 0, max_d = 0;
-  } learned[2];
+  // clique index: the local bitmaps of every root with 2 <= out-degree <= 256, built on the
+  // first clique call that can use it and kept with the device copy of the graph
+  int index_state = 0;              // 0 not built, 1 built, -1 over the memory budget
+  void* d_blocks = nullptr;
+  uint32_t* d_boff = nullptr;
+  std::vector<uint32_t> boff;       // host copy, rank space
+  size_t index_bytes = 0;
+  RootDesc* d_desc_deg = nullptr;   // task list of the descending-degree order (index counting)
+  // learned scheduler inputs on the device: base features per engine (0 = motifs, 1 =
+  // cliques) by original id, and the rank -> original id map of the DAG
+  float* d_feat[2] = {nullptr, nullptr};
+  int32_t* d_orig = nullptr;
 };
 
 static std::mutex g_dev_mu;
@@ -163,6 +178,12 @@ static void free_workspace(Workspace& w) {
   cudaFree(w.d_per_root);
   cudaFree(w.d_parts);
   cudaFree(w.d_bits);
+  cudaFree(w.d_desc);
+  cudaFree(w.d_params);
+  cudaFree(w.d_sched);
+  cudaFree(w.d_sroots);
+  cudaFree(w.d_sparts);
+  cudaFree(w.d_sdesc);
   if (w.ev0) cudaEventDestroy(w.ev0);
   if (w.ev1) cudaEventDestroy(w.ev1);
   if (w.k0) cudaEventDestroy(w.k0);
@@ -262,11 +283,13 @@ static int prepare_ws(Workspace& ws, cudaStream_t st) {
   return DM_OK;
 }
 
-// Initial counters: every root task is pending until a warp finishes it.
-static int init_counters(Workspace& ws, int n_roots, cudaStream_t st) {
+// Initial counters: every root task is pending until a warp finishes it; the root cursor
+// starts after the entries dealt statically.
+static int init_counters(Workspace& ws, int n_roots, cudaStream_t st, int cursor = 0) {
   DevCounters h;
   std::memset(&h, 0, sizeof(h));
   h.pending = n_roots;
+  h.cursor = cursor;
   DM_CUDA(cudaMemcpyAsync(ws.d_ctr, &h, sizeof(h), cudaMemcpyHostToDevice, st));
   return DM_OK;
 }
@@ -300,10 +323,12 @@ void release_device_graphs(dm_graph* g) {
       free_workspace(s->ws);
       cudaFree(s->d_deg_order);
       cudaFree(s->d_up_order);
-      for (auto& l : s->learned) {
-        cudaFree(l.d_roots);
-        cudaFree(l.d_parts);
-      }
+      cudaFree(s->d_blocks);
+      cudaFree(s->d_boff);
+      cudaFree(s->d_desc_deg);
+      cudaFree(s->d_feat[0]);
+      cudaFree(s->d_feat[1]);
+      cudaFree(s->d_orig);
       cudaSetDevice(cur);
     }
     cudaGetLastError();
@@ -326,7 +351,8 @@ int check_opts(const dm_opts* o) {
   if (!o) return DM_OK;
   if (o->struct_size != 0 && o->struct_size != (int32_t)sizeof(dm_opts))
     return fail(DM_EINVAL, "dm_opts.struct_size does not match this library");
-  if (o->mode < 0 || o->mode > 2) return fail(DM_EINVAL, "dm_opts.mode out of range");
+  if (o->mode < 0 || o->mode > 3) return fail(DM_EINVAL, "dm_opts.mode out of range");
+  if (o->staging < 0 || o->staging > 2) return fail(DM_EINVAL, "dm_opts.staging out of range");
   if (o->scheduler < 0 || o->scheduler > 2) return fail(DM_EINVAL, "dm_opts.scheduler out of range");
   if (o->vwarp != 0 && o->vwarp != 8 && o->vwarp != 16 && o->vwarp != 32)
     return fail(DM_EINVAL, "dm_opts.vwarp must be 0, 8, 16 or 32");
@@ -358,6 +384,73 @@ static int ensure_deg_order(dm_graph* g, DeviceSlot* s, cudaStream_t st) {
   return DM_OK;
 }
 
+static RootDesc root_desc(const dm_graph* g, const DeviceSlot* s, int32_t r, int32_t part) {
+  return RootDesc{r, (int32_t)(g->orow[r + 1] - g->orow[r]), s->boff.empty() ? INDEX_NONE : s->boff[r], part};
+}
+
+// Builds the clique index of this device copy (once): host block offsets, the device
+// blocks (index_build_kernel over the roots with 2 <= out-degree <= 256), and the task list
+// of the descending-degree order. Graphs whose index would exceed min(8 GB, a quarter of
+// the free device memory) keep rebuilding bitmaps per launch instead (index_state -1).
+static int ensure_index(dm_graph* g, DeviceSlot* s, LaunchCtx& ctx) {
+  if (s->index_state != 0) return DM_OK;
+  const int32_t n = g->n;
+  std::vector<uint32_t> boff((size_t)n, INDEX_NONE);
+  uint64_t total = 0;
+  int max_d = 0;
+  for (int32_t r = 0; r < n; ++r) {
+    const int d = (int)(g->orow[r + 1] - g->orow[r]);
+    if (d >= 2 && d <= INDEX_MAX_DEGREE) {
+      boff[r] = (uint32_t)total;
+      total += index_block_units_host(d);
+      max_d = std::max(max_d, d);
+    }
+  }
+  size_t free_b = 0, tot_b = 0;
+  DM_CUDA(cudaMemGetInfo(&free_b, &tot_b));
+  const size_t bytes = (size_t)total * 16;
+  if (total >= INDEX_NONE || bytes > std::min<size_t>((size_t)8 << 30, free_b / 4)) {
+    s->index_state = -1;
+    return DM_OK;
+  }
+  void* blocks = nullptr;
+  uint32_t* d_boff = nullptr;
+  RootDesc* desc = nullptr;
+  cudaError_t e = cudaMalloc(&blocks, std::max<size_t>(bytes, 16));
+  if (e == cudaSuccess) e = cudaMalloc(&d_boff, sizeof(uint32_t) * std::max(n, 1));
+  if (e == cudaSuccess) e = cudaMalloc(&desc, sizeof(RootDesc) * std::max(n, 1));
+  if (e != cudaSuccess) {
+    cudaFree(blocks);
+    cudaFree(d_boff);
+    cudaFree(desc);
+    cudaGetLastError();
+    s->index_state = -1;  // no room: per-launch bitmaps
+    return DM_OK;
+  }
+  s->boff.swap(boff);
+  std::vector<RootDesc> hd((size_t)n);
+  for (int32_t i = 0; i < n; ++i) hd[i] = root_desc(g, s, s->deg_order[i], 0);
+  s->d_blocks = blocks;
+  s->d_boff = d_boff;
+  s->d_desc_deg = desc;
+  s->index_bytes = bytes;
+  s->index_state = 1;
+  if (n) {
+    DM_CUDA(cudaMemcpyAsync(d_boff, s->boff.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice, ctx.stream));
+    DM_CUDA(cudaMemcpyAsync(desc, hd.data(), sizeof(RootDesc) * n, cudaMemcpyHostToDevice, ctx.stream));
+  }
+  // roots with out-degree in [2, 256] are a contiguous range of the descending-degree order
+  const int64_t lo = INDEX_MAX_DEGREE + 1 < (int64_t)s->cnt_ge.size() ? s->cnt_ge[INDEX_MAX_DEGREE + 1] : 0;
+  const int64_t hi = 2 < (int64_t)s->cnt_ge.size() ? s->cnt_ge[2] : 0;
+  const GraphView gv{s->dg.d_orow, s->dg.d_odeg, s->dg.d_oadj, n};
+  int rc = clique_index_build(gv, s->d_deg_order + lo, (int)(hi - lo), blocks, d_boff,
+                              std::max(1, (std::min(INDEX_MAX_DEGREE, max_d) + 63) / 64), ctx);
+  if (rc) return rc;
+  // the host vector must outlive the asynchronous copy
+  DM_CUDA(cudaStreamSynchronize(ctx.stream));
+  return DM_OK;
+}
+
 // Root order (shared by both engines): plain = descending degree (heaviest first), id =
 // ascending vertex id (the reference's round-robin striping order, DuMatoCPU.cu:126-135),
 // learned = descending predicted cost. The shard keeps every world_size-th task.
@@ -366,49 +459,59 @@ int predictor_schedule(const void* pv, dm_graph* g, int k, bool clique, int tota
 int ensure_features(dm_graph* g, bool clique);
 void predictor_key(const void* pv, uint64_t* uid, uint64_t* version);
 
-// Looks up (or fills) the cached learned schedule of this graph, device and engine.
-static bool learned_cached(DeviceSlot* s, int eng, int k, const dm_opts* o, const int32_t** roots,
-                           const int32_t** parts, int* n, int* max_d) {
-  uint64_t uid, ver;
-  predictor_key(o->predictor, &uid, &ver);
-  auto& l = s->learned[eng];
-  const int world = o->world_size > 1 ? o->world_size : 1, rank = world > 1 ? o->rank : 0;
-  if (!(l.valid && l.k == k && l.uid == uid && l.version == ver && l.world == world && l.rank == rank)) return false;
-  *roots = l.d_roots;
-  *parts = l.d_parts;
-  *n = l.n;
-  *max_d = l.max_d;
-  return true;
-}
-
-static int learned_store(DeviceSlot* s, int eng, int k, const dm_opts* o, const std::vector<int32_t>& roots,
-                         const std::vector<int32_t>& parts, int max_d, cudaStream_t st, const int32_t** d_roots,
-                         const int32_t** d_parts) {
-  auto& l = s->learned[eng];
-  l.valid = false;
-  const size_t n = std::max<size_t>(roots.size(), 1);
-  if (l.cap < n) {
-    cudaFree(l.d_roots);
-    cudaFree(l.d_parts);
-    l.d_roots = l.d_parts = nullptr;
-    l.cap = 0;
-    DM_CUDA(cudaMalloc(&l.d_roots, sizeof(int32_t) * n));
-    DM_CUDA(cudaMalloc(&l.d_parts, sizeof(int32_t) * n));
-    l.cap = n;
+// Runs the learned schedule on the device for the input entries in_roots[0..n_in) (device
+// pointer; rank space for cliques) and points *roots / *parts (and *desc for cliques on the
+// index) at the workspace's output task list of *n entries.
+static int learned_device(dm_graph* g, DeviceSlot* s, const dm_opts* o, int k, bool clique, const int32_t* in_roots,
+                          int n_in, LaunchCtx& ctx, const int32_t** roots, const int32_t** parts,
+                          const RootDesc** desc, int* n) {
+  Workspace& ws = s->ws;
+  const int eng = clique ? 1 : 0;
+  int rc;
+  if (!s->d_feat[eng]) {
+    const auto& F = g->feat[eng];
+    if (F.empty()) return fail(DM_EINVAL, "predictor features were not prepared");
+    DM_CUDA(cudaMalloc(&s->d_feat[eng], sizeof(float) * F.size()));
+    DM_CUDA(cudaMemcpyAsync(s->d_feat[eng], F.data(), sizeof(float) * F.size(), cudaMemcpyHostToDevice, ctx.stream));
   }
-  if (!roots.empty()) {
-    DM_CUDA(cudaMemcpyAsync(l.d_roots, roots.data(), sizeof(int32_t) * roots.size(), cudaMemcpyHostToDevice, st));
-    DM_CUDA(cudaMemcpyAsync(l.d_parts, parts.data(), sizeof(int32_t) * parts.size(), cudaMemcpyHostToDevice, st));
+  if (clique && !s->d_orig) {
+    std::vector<int32_t> inv(std::max(g->n, 1));
+    for (int32_t v = 0; v < g->n; ++v) inv[g->rank[v]] = v;
+    DM_CUDA(cudaMalloc(&s->d_orig, sizeof(int32_t) * inv.size()));
+    DM_CUDA(cudaMemcpyAsync(s->d_orig, inv.data(), sizeof(int32_t) * inv.size(), cudaMemcpyHostToDevice, ctx.stream));
+    DM_CUDA(cudaStreamSynchronize(ctx.stream));
   }
-  predictor_key(o->predictor, &l.uid, &l.version);
-  l.k = k;
-  l.world = o->world_size > 1 ? o->world_size : 1;
-  l.rank = l.world > 1 ? o->rank : 0;
-  l.n = (int)roots.size();
-  l.max_d = max_d;
-  l.valid = true;
-  *d_roots = l.d_roots;
-  *d_parts = l.d_parts;
+  const int warps = ctx.num_sms * 32;
+  const int cap = learned_schedule_cap(n_in, warps);
+  if ((rc = ensure_ws_bytes(reinterpret_cast<void**>(&ws.d_params), &ws.params_cap,
+                            sizeof(float) * predictor_num_params())) ||
+      (rc = ensure_ws_bytes(&ws.d_sched, &ws.sched_cap, learned_schedule_scratch_bytes(n_in))) ||
+      (rc = ensure_ws_bytes(reinterpret_cast<void**>(&ws.d_sroots), &ws.sroots_cap, sizeof(int32_t) * cap)) ||
+      (rc = ensure_ws_bytes(reinterpret_cast<void**>(&ws.d_sparts), &ws.sparts_cap, sizeof(int32_t) * cap)))
+    return rc;
+  const bool with_desc = clique && s->index_state == 1;
+  if (with_desc &&
+      (rc = ensure_ws_bytes(reinterpret_cast<void**>(&ws.d_sdesc), &ws.sdesc_cap, sizeof(RootDesc) * cap)))
+    return rc;
+  SchedIO io;
+  io.feat = s->d_feat[eng];
+  io.params = ws.d_params;
+  io.roots = in_roots;
+  io.orig = clique ? s->d_orig : nullptr;
+  io.n_in = n_in;
+  io.k = k;
+  io.warps = warps;
+  io.cap = cap;
+  io.scratch = ws.d_sched;
+  io.out_roots = ws.d_sroots;
+  io.out_parts = ws.d_sparts;
+  io.out_desc = with_desc ? ws.d_sdesc : nullptr;
+  io.odeg = s->dg.d_odeg;
+  io.boff = with_desc ? s->d_boff : nullptr;
+  if ((rc = learned_schedule_device(o->predictor, io, ctx, n))) return rc;
+  *roots = ws.d_sroots;
+  *parts = ws.d_sparts;
+  if (desc) *desc = with_desc ? ws.d_sdesc : nullptr;
   return DM_OK;
 }
 
@@ -416,10 +519,7 @@ static int order_roots(dm_graph* g, const dm_opts* o, int k, bool clique, int to
                        std::vector<int32_t>& roots, std::vector<int32_t>& parts) {
   const int sched = o ? o->scheduler : DM_SCHED_PLAIN;
   parts.clear();
-  if (sched == DM_SCHED_LEARNED) {
-    int rc = predictor_schedule(o->predictor, g, k, clique, total_warps, roots, parts);
-    if (rc) return rc;
-  } else if (sched == DM_SCHED_ID) {
+  if (sched == DM_SCHED_ID) {
     if (clique) {
       // rank space -> ascending original id
       std::vector<int32_t> inv(g->n);
@@ -443,14 +543,12 @@ static int order_roots(dm_graph* g, const dm_opts* o, int k, bool clique, int to
     }
   }
   if (o && o->world_size > 1) {
-    std::vector<int32_t> mine, mparts;
-    for (size_t i = o->rank; i < roots.size(); i += o->world_size) {
-      mine.push_back(roots[i]);
-      if (!parts.empty()) mparts.push_back(parts[i]);
-    }
+    std::vector<int32_t> mine;
+    for (size_t i = o->rank; i < roots.size(); i += o->world_size) mine.push_back(roots[i]);
     roots.swap(mine);
-    parts.swap(mparts);
   }
+  // the learned schedule reorders and splits the shard of the plain order
+  if (sched == DM_SCHED_LEARNED) return predictor_schedule(o->predictor, g, k, clique, total_warps, roots, parts);
   return DM_OK;
 }
 
@@ -502,18 +600,44 @@ int dm_count_cliques(dm_graph* g, int32_t k, const dm_opts* o, uint64_t* count, 
   const int sched = o ? o->scheduler : DM_SCHED_PLAIN;
   const int world = (o && o->world_size > 1) ? o->world_size : 1;
   if ((rc = ensure_deg_order(g, s, ctx.stream))) return rc;
+  const int mode = o ? o->mode : DM_MODE_AUTO;
+  const bool want_index = (mode == DM_MODE_AUTO || mode == DM_MODE_BITMAP) && k >= 3 && k <= INDEX_MAX_K;
+  if (want_index && (rc = ensure_index(g, s, ctx))) return rc;
   std::vector<int32_t> roots, parts;
   const int32_t* d_roots = nullptr;
+  const RootDesc* d_desc = nullptr;
   int n_roots = 0, max_d = 0;
   if (sched == DM_SCHED_PLAIN && world == 1) {
     // the eligible roots are a prefix of the cached descending-degree order
     n_roots = need <= g->max_out_degree ? (int)s->cnt_ge[need] : 0;
     d_roots = s->d_deg_order;
+    d_desc = s->d_desc_deg;
     max_d = n_roots ? (int)(g->orow[s->deg_order[0] + 1] - g->orow[s->deg_order[0]]) : 0;
   }
   const int32_t* d_parts = nullptr;
   if (d_roots) {
-  } else if (sched == DM_SCHED_LEARNED && learned_cached(s, 1, k, o, &d_roots, &d_parts, &n_roots, &max_d)) {
+  } else if (sched == DM_SCHED_LEARNED) {
+    // the plain order (this shard of it), reordered and split by the schedule on the device
+    const int32_t* in = s->d_deg_order;
+    int n_in = need <= g->max_out_degree ? (int)s->cnt_ge[need] : 0;
+    if (n_in) max_d = (int)(g->orow[s->deg_order[0] + 1] - g->orow[s->deg_order[0]]);
+    if (world > 1) {
+      dm_opts po = *o;
+      po.scheduler = DM_SCHED_PLAIN;
+      for (int32_t r = 0; r < g->n; ++r)
+        if (g->orow[r + 1] - g->orow[r] >= need) roots.push_back(r);
+      if ((rc = order_roots(g, &po, k, true, ctx.num_sms * 32, roots, parts))) return rc;
+      max_d = roots.empty() ? 0 : (int)(g->orow[roots[0] + 1] - g->orow[roots[0]]);
+      if ((rc = ensure_ws_bytes(reinterpret_cast<void**>(&ws.d_tasks), &ws.tasks_cap,
+                                sizeof(int32_t) * (roots.size() + 1))))
+        return rc;
+      if (!roots.empty())
+        DM_CUDA(cudaMemcpyAsync(ws.d_tasks, roots.data(), sizeof(int32_t) * roots.size(), cudaMemcpyHostToDevice,
+                                ctx.stream));
+      in = ws.d_tasks;
+      n_in = (int)roots.size();
+    }
+    if ((rc = learned_device(g, s, o, k, true, in, n_in, ctx, &d_roots, &d_parts, &d_desc, &n_roots))) return rc;
   } else {
     roots.reserve(g->n);
     for (int32_t r = 0; r < g->n; ++r)
@@ -521,13 +645,22 @@ int dm_count_cliques(dm_graph* g, int32_t k, const dm_opts* o, uint64_t* count, 
     if ((rc = order_roots(g, o, k, true, ctx.num_sms * 32, roots, parts))) return rc;
     for (int32_t r : roots) max_d = std::max(max_d, (int)(g->orow[r + 1] - g->orow[r]));
     n_roots = (int)roots.size();
-    if (sched == DM_SCHED_LEARNED) {
-      if ((rc = learned_store(s, 1, k, o, roots, parts, max_d, ctx.stream, &d_roots, &d_parts))) return rc;
-    } else if ((rc = upload_parts(ws, parts, ctx.stream, &d_parts))) {
-      return rc;
+    {
+      if ((rc = upload_parts(ws, parts, ctx.stream, &d_parts))) return rc;
+      if (s->index_state == 1) {
+        std::vector<RootDesc> hd(roots.size());
+        for (size_t i = 0; i < roots.size(); ++i) hd[i] = root_desc(g, s, roots[i], parts.empty() ? 0 : parts[i]);
+        if ((rc = ensure_ws_bytes(reinterpret_cast<void**>(&ws.d_desc), &ws.desc_cap,
+                                  sizeof(RootDesc) * (hd.size() + 1))))
+          return rc;
+        if (!hd.empty())
+          DM_CUDA(cudaMemcpyAsync(ws.d_desc, hd.data(), sizeof(RootDesc) * hd.size(), cudaMemcpyHostToDevice,
+                                  ctx.stream));
+        d_desc = ws.d_desc;
+      }
     }
   }
-  const int mode = o ? o->mode : DM_MODE_AUTO;
+  const bool use_index = want_index && s->index_state == 1 && d_desc != nullptr;
   CliqueLaunch L;
   L.k = k;
   if (mode == DM_MODE_LIST) {
@@ -563,7 +696,6 @@ int dm_count_cliques(dm_graph* g, int32_t k, const dm_opts* o, uint64_t* count, 
     DM_CUDA(cudaMemsetAsync(ws.d_per_root, 0, sizeof(unsigned long long) * std::max(g->n, 1), ctx.stream));
     L.per_root = ws.d_per_root;
   }
-  if ((rc = init_counters(ws, n_roots, ctx.stream))) return rc;
   L.g = GraphView{s->dg.d_orow, s->dg.d_odeg, s->dg.d_oadj, g->n};
   L.roots = d_roots;
   L.parts = d_parts;
@@ -573,10 +705,25 @@ int dm_count_cliques(dm_graph* g, int32_t k, const dm_opts* o, uint64_t* count, 
   L.qcap = ws.qcap;
   L.nq = QUEUE_SHARDS;
   L.max_donations = ctx.donations_per_warp;
+  int grid = 0, cursor = 0;
+  if (use_index) {
+    L.desc = d_desc;
+    L.blocks = s->d_blocks;
+    L.boff = s->d_boff;
+    L.tma = !(o && o->staging == DM_STAGE_LOADS);
+    if (n_roots > 0) {
+      if ((rc = clique_cached_grid(L, ctx, &grid))) return rc;
+      // every warp starts on a static chunk of the list: no cursor atomics at launch
+      const int warps = grid * 8;
+      L.static_chunk = std::max(1, std::min(8, n_roots / std::max(warps, 1)));
+      L.n_static = (int)std::min<int64_t>(n_roots, (int64_t)warps * L.static_chunk);
+      cursor = L.n_static;
+    }
+  }
+  if ((rc = init_counters(ws, n_roots, ctx.stream, cursor))) return rc;
   DM_CUDA(cudaEventRecord(ws.k0, ctx.stream));
-  int grid = 0;
   if (n_roots > 0) {
-    rc = clique_launch(L, ctx, &grid);
+    rc = use_index ? clique_cached_launch(L, ctx, grid) : clique_launch(L, ctx, &grid);
     if (rc) return rc;
   }
   DM_CUDA(cudaEventRecord(ws.k1, ctx.stream));
@@ -608,7 +755,7 @@ int dm_count_cliques(dm_graph* g, int32_t k, const dm_opts* o, uint64_t* count, 
     st->donations = h.donations;
     st->idle_polls = h.idle_polls;
     st->nodes = h.nodes;
-    st->mode_used = mode == DM_MODE_LIST ? DM_MODE_LIST : DM_MODE_BITMAP;
+    st->mode_used = mode == DM_MODE_LIST ? DM_MODE_LIST : (use_index ? DM_MODE_BITMAP : DM_MODE_REBUILD);
     st->vwarp_used = 32;
     st->grid = grid;
     st->block = 256;
@@ -667,20 +814,36 @@ int dm_count_motifs(dm_graph* g, int32_t k, const dm_dictionary* dict, const dm_
   }
   std::vector<int32_t> roots, parts;
   const int32_t* d_parts_cached = nullptr;
-  int max_d_unused = 0;
   if (sched == DM_SCHED_PLAIN && world == 1) {
     d_roots = s->d_up_order;
     n_roots = s->n_up;
-  } else if (sched == DM_SCHED_LEARNED && learned_cached(s, 0, k, o, &d_roots, &d_parts_cached, &n_roots,
-                                                         &max_d_unused)) {
+  } else if (sched == DM_SCHED_LEARNED) {
+    // the plain order (this shard of it), reordered and split by the schedule on the device
+    const int32_t* in = s->d_up_order;
+    int n_in = s->n_up;
+    if (world > 1) {
+      dm_opts po = *o;
+      po.scheduler = DM_SCHED_PLAIN;
+      for (int32_t v = 0; v < g->n; ++v)
+        if (upper(v) > 0) roots.push_back(v);
+      if ((rc = order_roots(g, &po, k, false, ctx.num_sms * 32, roots, parts))) return rc;
+      if ((rc = ensure_ws_bytes(reinterpret_cast<void**>(&ws.d_tasks), &ws.tasks_cap,
+                                sizeof(int32_t) * (roots.size() + 1))))
+        return rc;
+      if (!roots.empty())
+        DM_CUDA(cudaMemcpyAsync(ws.d_tasks, roots.data(), sizeof(int32_t) * roots.size(), cudaMemcpyHostToDevice,
+                                ctx.stream));
+      in = ws.d_tasks;
+      n_in = (int)roots.size();
+    }
+    if ((rc = learned_device(g, s, o, k, false, in, n_in, ctx, &d_roots, &d_parts_cached, nullptr, &n_roots)))
+      return rc;
   } else {
     for (int32_t v = 0; v < g->n; ++v)
       if (upper(v) > 0) roots.push_back(v);
     if ((rc = order_roots(g, o, k, false, ctx.num_sms * 32, roots, parts))) return rc;
     n_roots = (int)roots.size();
-    if (sched == DM_SCHED_LEARNED) {
-      if ((rc = learned_store(s, 0, k, o, roots, parts, 0, ctx.stream, &d_roots, &d_parts_cached))) return rc;
-    } else {
+    {
       if ((rc = ensure_ws_bytes(reinterpret_cast<void**>(&ws.d_tasks), &ws.tasks_cap,
                                 sizeof(int32_t) * (roots.size() + 1))))
         return rc;

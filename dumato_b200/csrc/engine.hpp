@@ -72,6 +72,51 @@ struct LaunchCtx {
   int test_stall = 0;        // DM_TEST_STALL_AT_EXIT
 };
 
+// Clique index (clique_cached.cuh): the local adjacency bitmap of every root r of the DAG
+// with 2 <= d = |N+(r)| <= 256, as d rows of ceil(d/64) u64 words, the block starting on a
+// 16-byte boundary (offset in 16-byte units; INDEX_NONE for roots without a block).
+constexpr uint32_t INDEX_NONE = 0xffffffffu;
+constexpr int INDEX_MAX_DEGREE = 256;
+constexpr int INDEX_MAX_K = 8;  // larger k rebuild the bitmaps per launch
+
+inline uint32_t index_block_units_host(int d) {
+  const int nw = (d + 63) >> 6;
+  return (uint32_t)((d * nw + 1) >> 1);
+}
+
+// One entry of a counting launch's task list on the index: root (rank space), out-degree,
+// block offset (16-byte units, or INDEX_NONE) and scheduler part word (p | P << 16, 0 = whole).
+struct RootDesc {
+  int32_t root;
+  int32_t d;
+  uint32_t off;
+  int32_t part;
+};
+
+// Scheduler part words: p | P << 16 (part p of P; 0 = the whole root), plus PART_EAGER when
+// the learned scheduler predicts the task to be heavy, so that it donates without waiting
+// for the minimum task age.
+constexpr int PART_EAGER = 1 << 30;
+
+// The learned schedule on the device (predictor.cu): inputs, scratch and outputs.
+struct SchedIO {
+  const float* feat = nullptr;       // n x 6 base features by original id
+  float* params = nullptr;           // MLP parameters (written by the call)
+  const int32_t* roots = nullptr;    // n_in input entries
+  const int32_t* orig = nullptr;     // rank -> original id (cliques), else null
+  int n_in = 0, k = 0, warps = 1, cap = 0;
+  void* scratch = nullptr;           // learned_schedule_scratch_bytes(n_in)
+  int32_t* out_roots = nullptr;      // cap
+  int32_t* out_parts = nullptr;      // cap
+  RootDesc* out_desc = nullptr;      // cap or null
+  const int32_t* odeg = nullptr;     // rank-space out-degrees (out_desc)
+  const uint32_t* boff = nullptr;    // index block offsets (out_desc), or null
+};
+int learned_schedule_device(const void* predictor, const SchedIO& io, LaunchCtx& ctx, int* n_out);
+size_t learned_schedule_scratch_bytes(int n_in);
+inline int learned_schedule_cap(int n_in, int warps) { return n_in + 4 * warps + 64; }
+int predictor_num_params();
+
 // Clique engine (clique.cu).
 struct CliqueLaunch {
   GraphView g;                   // degree-ordered DAG in rank space
@@ -89,9 +134,23 @@ struct CliqueLaunch {
   int nwmax = 1;
   unsigned long long* per_root = nullptr;
   const int32_t* parts = nullptr;   // per root entry: p | P << 16 (0 = whole root)
+  // counting on the clique index (clique_cached_*), else the per-launch bitmap build
+  const RootDesc* desc = nullptr;   // task list (n_roots entries)
+  const void* blocks = nullptr;     // the index (16-byte units)
+  const uint32_t* boff = nullptr;   // block offset per root
+  int static_chunk = 1;             // warp w starts with entries [w * static_chunk, +static_chunk)
+  int n_static = 0;                 // entries dealt statically; the root cursor starts here
+  bool tma = true;                  // stage blocks by bulk asynchronous copies (else 16-byte loads)
 };
 int clique_launch(const CliqueLaunch& L, LaunchCtx& ctx, int* grid);
 int clique_max_warps(int num_sms);
+// Grid of the index-counting kernel for this launch (occupancy, requested threads, arena).
+int clique_cached_grid(const CliqueLaunch& L, LaunchCtx& ctx, int* grid);
+// Counting on the index with that grid (L.static_chunk / L.n_static set for it).
+int clique_cached_launch(const CliqueLaunch& L, LaunchCtx& ctx, int grid);
+// Builds the index blocks of roots[0..n) (rank space, 2 <= out-degree <= 64 * m).
+int clique_index_build(const GraphView& g, const int32_t* roots, int n, void* blocks, const uint32_t* boff, int m,
+                       LaunchCtx& ctx);
 
 // Motif engine (motif.cu).
 struct MotifLaunch {

@@ -1,5 +1,6 @@
-// Device-side GPM step library: the warp-level building blocks the enumeration kernels are
-// written in (the role of the reference's DuMatoGPU class, src/main/DuMatoGPU.cu).
+// Internal warp-level helpers of the enumeration kernels. The public step library (extend,
+// filter, compact, aggregate; include/dumato_b200_gpm.cuh) is included here; the helpers
+// below add explicit-mask forms used where a group mask is already at hand.
 //
 //   compact  - stable warp stream compaction by ballot + popc: the valid lanes of a 32-wide
 //              chunk land in lane order at the list tail (DuMatoGPU.cu:317-343 write /
@@ -14,6 +15,8 @@
 #pragma once
 
 #include <cstdint>
+
+#include "dumato_b200_gpm.cuh"
 
 namespace dmb {
 

@@ -170,9 +170,12 @@ static __device__ __noinline__ bool q_pop(const LBArgs& lb, int home, int& root,
 
 // Lane-0 only. Claims a chunk of roots [first, first+count) from the cursor, or failing
 // that a donated task (count = 1, range [b, e)). Returns false when all work is done or an
-// error was raised.
+// error was raised. A caller that defers the pending-count decrements of the roots it has
+// finished passes their number in *unflushed: they are subtracted before the caller waits
+// for work (so `pending` can reach zero), and *unflushed is reset.
 static __device__ __noinline__ bool lb_next(const LBArgs& lb, int n_roots, int total_warps, int& first, int& count,
-                                            int& b, int& e, bool& donated, int& level, int* path) {
+                                            int& b, int& e, bool& donated, int& level, int* path,
+                                            int* unflushed = nullptr) {
   DevCounters* c = lb.ctr;
   int cur = vload(&c->cursor);
   if (cur < n_roots) {
@@ -189,6 +192,11 @@ static __device__ __noinline__ bool lb_next(const LBArgs& lb, int n_roots, int t
       donated = false;
       return true;
     }
+  }
+  if (unflushed && *unflushed) {
+    __threadfence();
+    atomicSub(&c->pending, *unflushed);
+    *unflushed = 0;
   }
   atomicAdd(&c->hungry, 1);
   const long long t_hungry = global_ns();
@@ -267,11 +275,12 @@ __device__ __forceinline__ void task_range(int b, int e, int n, int& lo, int& hi
   }
 }
 
-// Decodes a scheduler part word (p | P << 16; 0 = the whole root) into (b, e).
+// Decodes a scheduler part word into (b, e).
 __device__ __forceinline__ void part_bounds(int part, int& b, int& e) {
-  if (part) {
-    b = -1 - (part & 0xffff);
-    e = -1 - (part >> 16);
+  const int pp = part & ~PART_EAGER;
+  if (pp) {
+    b = -1 - (pp & 0xffff);
+    e = -1 - ((pp >> 16) & 0x3fff);
   }
 }
 
@@ -309,13 +318,14 @@ __device__ __forceinline__ int split_mid(int next, int end, int cost_tail) {
 // cannot simply be undone). `busy` serialises donations of one warp.
 __device__ __forceinline__ bool range_maybe_donate(const LBArgs& lb, unsigned long long* range, int root,
                                                    int* donations_left, long long task_start, int* busy, int& ob,
-                                                   int& oe, int cost_tail = 0, int min_items = 0) {
+                                                   int& oe, int cost_tail = 0, int min_items = 0, int level = 0,
+                                                   const int* path = nullptr, bool eager = false) {
   if (lb.hungry_trigger <= 0) return false;
   if (*reinterpret_cast<volatile int*>(donations_left) <= 0) return false;
   // demand: hungry warps not yet served by a queued task
   const int hungry = vload(&lb.ctr->hungry);
   if (hungry - vload(&lb.ctr->queued) < lb.hungry_trigger) return false;
-  if (global_ns() - task_start < lb.donate_after_ns) return false;
+  if (!eager && global_ns() - task_start < lb.donate_after_ns) return false;
   if (atomicCAS(busy, 0, 1) != 0) return false;
   bool own = false;
   unsigned long long cur = *reinterpret_cast<volatile unsigned long long*>(range);
@@ -331,9 +341,10 @@ __device__ __forceinline__ bool range_maybe_donate(const LBArgs& lb, unsigned lo
     }
     atomicAdd(&lb.ctr->pending, 1);
     const int home = (int)((blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) % (unsigned)lb.nq);
-    if (q_push(lb, home, root, mid, end, 0, nullptr)) {
+    if (q_push(lb, home, root, mid, end, level, path)) {
       atomicSub(donations_left, 1);
       atomicAdd(&lb.ctr->donations, 1ull);
+      if (level > 0) atomicAdd(&lb.ctr->prefix_donations, 1ull);
     } else {
       atomicSub(&lb.ctr->pending, 1);
       ob = mid;

@@ -146,14 +146,10 @@ __device__ __forceinline__ bool in_runs(int32_t x, const int32_t* run0, int n0, 
 // Adds the masks of list[lo, hi) to the group's 32-entry histogram h (aggregated per mask).
 template <int W>
 __device__ __forceinline__ void mask_hist(const int2* list, int lo, int hi, unsigned* h, int gl, unsigned gmask) {
-  const int lane = lane_id();
   for (int i0 = lo; i0 < hi; i0 += W) {
     const int i = i0 + gl;
     const bool v = i < hi;
-    const int m = v ? list[i].y : -1;
-    const unsigned act = __ballot_sync(gmask, v);
-    const unsigned same = __match_any_sync(gmask, m);
-    if (v && (same & act & ((1u << lane) - 1u)) == 0) atomicAdd(&h[m], (unsigned)__popc(same & act));
+    dm_gpm::aggregate_pattern<W>(h, v ? list[i].y : 0, v);
   }
   __syncwarp(gmask);
 }

@@ -62,16 +62,9 @@ void predictor_key(const void* pv, uint64_t* uid, uint64_t* version) {
   *version = p->version;
 }
 
-__global__ void mlp_forward_kernel(const float* __restrict__ P, const float* __restrict__ X, int n,
-                                   float* __restrict__ y) {
-  __shared__ float sp[MLP_NP];
-  for (int i = threadIdx.x; i < MLP_NP; i += blockDim.x) sp[i] = P[i];
-  __syncthreads();
-  const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= n) return;
-  float x[MLP_F], h1[MLP_H];
-#pragma unroll
-  for (int f = 0; f < MLP_F; ++f) x[f] = X[(size_t)s * MLP_F + f];
+// MLP forward of one feature row, parameters in shared memory.
+__device__ __forceinline__ float mlp_eval(const float* sp, const float* x) {
+  float h1[MLP_H];
 #pragma unroll
   for (int h = 0; h < MLP_H; ++h) {
     float a = sp[OFF_B1 + h];
@@ -86,7 +79,20 @@ __global__ void mlp_forward_kernel(const float* __restrict__ P, const float* __r
     for (int j = 0; j < MLP_H; ++j) a = fmaf(sp[OFF_W2 + h * MLP_H + j], h1[j], a);
     out = fmaf(sp[OFF_W3 + h], fmaxf(a, 0.f), out);
   }
-  y[s] = out;
+  return out;
+}
+
+__global__ void mlp_forward_kernel(const float* __restrict__ P, const float* __restrict__ X, int n,
+                                   float* __restrict__ y) {
+  __shared__ float sp[MLP_NP];
+  for (int i = threadIdx.x; i < MLP_NP; i += blockDim.x) sp[i] = P[i];
+  __syncthreads();
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  float x[MLP_F];
+#pragma unroll
+  for (int f = 0; f < MLP_F; ++f) x[f] = X[(size_t)s * MLP_F + f];
+  y[s] = mlp_eval(sp, x);
 }
 
 // Gradients of mean squared error over the samples idx[0..n) (or 0..n when idx is null).
@@ -336,8 +342,182 @@ static int predict_rows(const dm_predictor* p, const float* X, int64_t n, float*
   return DM_OK;
 }
 
-// Learned schedule: roots ordered by predicted cost (descending); a root whose predicted
-// cost exceeds a warp's fair share is split into up to 64 parts (p | P << 16 part words).
+// ---------------- the learned schedule on the device ----------------
+//
+// For the n_in root entries of a launch (the plain order, or one shard of it): the feature
+// row of each root is assembled from the cached per-vertex base features, the MLP predicts
+// log(1 + subtree size), and
+//   cost = expm1(prediction) and a descending log-cost bucket (1/64 per bucket);
+//   P = parts of the root: 1, or min(64, ceil(4 cost / share)) when the cost exceeds one
+//       warp's share (total cost / warps);
+//   the entries are written longest-first by a counting sort over the buckets (order inside
+//   a bucket is arbitrary), each root as P consecutive entries (p | P << 16), flagged
+//   PART_EAGER when its predicted cost is above EAGER_SHARE x share, so that the counting
+//   kernel donates from it without waiting for the minimum task age.
+// No allocation per call: the scratch lives in the caller's workspace.
+constexpr int SCHED_BINS = 2048;
+constexpr float EAGER_SHARE = 0.25f;
+
+struct SchedArgs {
+  const float* feat;        // n x BASE_F base features by original id
+  const float* params;      // MLP_NP
+  const int32_t* roots;     // n_in entries: rank space (cliques) or vertex ids (motifs)
+  const int32_t* orig;      // rank -> original id (cliques), else null
+  int n_in, k, warps, cap;
+  float* cost;              // n_in
+  int* bin;                 // n_in
+  int* nparts;              // n_in
+  double* total;            // 1
+  unsigned* bins;           // SCHED_BINS
+  int* n_out;               // 1
+  int* err;                 // 1 (set when the output capacity would be exceeded)
+  int32_t* out_roots;       // cap
+  int32_t* out_parts;       // cap
+  RootDesc* out_desc;       // cap, or null (cliques on the index)
+  const int32_t* odeg;      // rank-space out-degrees (out_desc)
+  const uint32_t* boff;     // index block offsets (out_desc)
+};
+
+__global__ void __launch_bounds__(256) sched_predict_kernel(SchedArgs a) {
+  __shared__ float sp[MLP_NP];
+  __shared__ double red[8];
+  for (int i = threadIdx.x; i < MLP_NP; i += blockDim.x) sp[i] = a.params[i];
+  __syncthreads();
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double c = 0.0;
+  if (i < a.n_in) {
+    const int32_t r = a.roots[i];
+    const int32_t v = a.orig ? a.orig[r] : r;
+    const float* b = a.feat + (size_t)v * BASE_F;
+    const float x[MLP_F] = {b[0], b[1], b[2], a.k / 8.f, (a.k - 2) / 8.f, b[3], b[4], b[5]};
+    const float y = fminf(fmaxf(mlp_eval(sp, x), 0.f), 40.f);
+    c = (double)expm1f(y);
+    a.cost[i] = (float)c;
+    a.bin[i] = SCHED_BINS - 1 - min(SCHED_BINS - 1, (int)(y * 64.f));
+  }
+  for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = c;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+    atomicAdd(a.total, t);
+  }
+}
+
+__global__ void __launch_bounds__(256) sched_parts_kernel(SchedArgs a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.n_in) return;
+  const double share = *a.total / (double)max(1, a.warps);
+  const double c = (double)a.cost[i];
+  int P = 1;
+  if (share > 0 && c > share) P = (int)fmin(64.0, ceil(4.0 * c / share));
+  a.nparts[i] = P;
+  atomicAdd(a.bins + a.bin[i], (unsigned)P);
+}
+
+// Exclusive scan of the bucket counts (one block of 1024 threads, two buckets per thread).
+__global__ void __launch_bounds__(1024) sched_scan_kernel(SchedArgs a) {
+  __shared__ unsigned part[1024];
+  const int t = threadIdx.x;
+  const unsigned c0 = a.bins[2 * t], c1 = a.bins[2 * t + 1];
+  part[t] = c0 + c1;
+  __syncthreads();
+  for (int o = 1; o < 1024; o <<= 1) {
+    const unsigned y = t >= o ? part[t - o] : 0u;
+    __syncthreads();
+    part[t] += y;
+    __syncthreads();
+  }
+  const unsigned excl = part[t] - (c0 + c1);
+  a.bins[2 * t] = excl;
+  a.bins[2 * t + 1] = excl + c0;
+  if (t == 1023) *a.n_out = (int)part[t];
+}
+
+__global__ void __launch_bounds__(256) sched_scatter_kernel(SchedArgs a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.n_in) return;
+  const int P = a.nparts[i];
+  const unsigned pos = atomicAdd(a.bins + a.bin[i], (unsigned)P);
+  if ((long long)pos + P > a.cap) {
+    atomicExch(a.err, 1);
+    return;
+  }
+  const int32_t r = a.roots[i];
+  const double share = *a.total / (double)max(1, a.warps);
+  const int eager = share > 0 && (double)a.cost[i] > EAGER_SHARE * share ? PART_EAGER : 0;
+  for (int q = 0; q < P; ++q) {
+    const int32_t pw = (P > 1 ? (q | (P << 16)) : 0) | eager;
+    a.out_roots[pos + q] = r;
+    a.out_parts[pos + q] = pw;
+    if (a.out_desc) a.out_desc[pos + q] = RootDesc{r, a.odeg[r], a.boff ? a.boff[r] : INDEX_NONE, pw};
+  }
+}
+
+// Runs the schedule of `in` (device root entries) on ctx.stream into the scratch `w`, and
+// returns the number of output entries (a 4-byte read-back). Output capacity: n_in + 4 x
+// warps + 64 entries (the parts of the roots above one share sum to at most 4 x warps +
+// their count).
+int learned_schedule_device(const void* pv, const SchedIO& io, LaunchCtx& ctx, int* n_out) {
+  const dm_predictor* p = reinterpret_cast<const dm_predictor*>(pv);
+  SchedArgs a;
+  a.feat = io.feat;
+  a.params = io.params;
+  a.roots = io.roots;
+  a.orig = io.orig;
+  a.n_in = io.n_in;
+  a.k = io.k;
+  a.warps = io.warps;
+  a.cap = io.cap;
+  char* w = reinterpret_cast<char*>(io.scratch);
+  auto take = [&](size_t bytes) {
+    char* q = w;
+    w += (bytes + 255) / 256 * 256;
+    return q;
+  };
+  a.total = reinterpret_cast<double*>(take(sizeof(double)));
+  a.n_out = reinterpret_cast<int*>(take(sizeof(int)));
+  a.err = reinterpret_cast<int*>(take(sizeof(int)));
+  a.bins = reinterpret_cast<unsigned*>(take(sizeof(unsigned) * SCHED_BINS));
+  a.cost = reinterpret_cast<float*>(take(sizeof(float) * std::max(io.n_in, 1)));
+  a.bin = reinterpret_cast<int*>(take(sizeof(int) * std::max(io.n_in, 1)));
+  a.nparts = reinterpret_cast<int*>(take(sizeof(int) * std::max(io.n_in, 1)));
+  a.out_roots = io.out_roots;
+  a.out_parts = io.out_parts;
+  a.out_desc = io.out_desc;
+  a.odeg = io.odeg;
+  a.boff = io.boff;
+  // the scratch header (total, n_out, err, bins) starts at zero
+  DM_CUDA(cudaMemsetAsync(io.scratch, 0, (size_t)(reinterpret_cast<char*>(a.cost) - reinterpret_cast<char*>(io.scratch)),
+                          ctx.stream));
+  DM_CUDA(cudaMemcpyAsync(io.params, p->params.data(), sizeof(float) * MLP_NP,
+                          cudaMemcpyHostToDevice, ctx.stream));
+  const unsigned grid = (unsigned)std::max(1, (io.n_in + 255) / 256);
+  sched_predict_kernel<<<grid, 256, 0, ctx.stream>>>(a);
+  sched_parts_kernel<<<grid, 256, 0, ctx.stream>>>(a);
+  sched_scan_kernel<<<1, 1024, 0, ctx.stream>>>(a);
+  sched_scatter_kernel<<<grid, 256, 0, ctx.stream>>>(a);
+  ctx.launches += 4;
+  DM_CUDA(cudaGetLastError());
+  int hdr[2] = {0, 0};
+  DM_CUDA(cudaMemcpyAsync(&hdr[0], a.n_out, sizeof(int), cudaMemcpyDeviceToHost, ctx.stream));
+  DM_CUDA(cudaMemcpyAsync(&hdr[1], a.err, sizeof(int), cudaMemcpyDeviceToHost, ctx.stream));
+  DM_CUDA(cudaStreamSynchronize(ctx.stream));
+  if (hdr[1]) return fail(DM_EINTERNAL, "learned schedule exceeded its output capacity");
+  *n_out = hdr[0];
+  return DM_OK;
+}
+
+int predictor_num_params() { return MLP_NP; }
+
+size_t learned_schedule_scratch_bytes(int n_in) {
+  const size_t n = (size_t)std::max(n_in, 1);
+  return 4 * 256 + (sizeof(unsigned) * SCHED_BINS + 255) / 256 * 256 + 3 * ((n * 4 + 255) / 256 * 256);
+}
+
+// Host version of the same schedule, for planning (dm_plan_roots): same costs, parts and
+// flags, with ties inside a bucket in input order.
 int predictor_schedule(const void* pv, dm_graph* g, int k, bool clique, int total_warps, std::vector<int32_t>& roots,
                        std::vector<int32_t>& parts) {
   const dm_predictor* p = reinterpret_cast<const dm_predictor*>(pv);
@@ -357,16 +537,17 @@ int predictor_schedule(const void* pv, dm_graph* g, int k, bool clique, int tota
   std::vector<float> pred(roots.size());
   if ((rc = predict_rows(p, Xr.data(), (int64_t)roots.size(), pred.data()))) return rc;
   std::vector<double> cost(roots.size());
+  std::vector<int> bin(roots.size());
   double total = 0;
   for (size_t i = 0; i < roots.size(); ++i) {
-    cost[i] = std::expm1(std::min<double>(std::max<double>(pred[i], 0.0), 40.0));
+    const float y = std::min(std::max(pred[i], 0.f), 40.f);
+    cost[i] = (double)std::expm1(y);
+    bin[i] = SCHED_BINS - 1 - std::min(SCHED_BINS - 1, (int)(y * 64.f));
     total += cost[i];
   }
   std::vector<size_t> order(roots.size());
   std::iota(order.begin(), order.end(), 0);
-  std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) { return cost[a] > cost[b]; });
-  // a root predicted to cost more than one warp's fair share is split so that each part is
-  // about a quarter of that share
+  std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) { return bin[a] < bin[b]; });
   const double share = total / std::max(1, total_warps);
   std::vector<int32_t> out_roots, out_parts;
   out_roots.reserve(roots.size());
@@ -374,9 +555,10 @@ int predictor_schedule(const void* pv, dm_graph* g, int k, bool clique, int tota
   for (size_t i : order) {
     int P = 1;
     if (share > 0 && cost[i] > share) P = (int)std::min<double>(64.0, std::ceil(4.0 * cost[i] / share));
+    const int eager = share > 0 && cost[i] > EAGER_SHARE * share ? PART_EAGER : 0;
     for (int q = 0; q < P; ++q) {
       out_roots.push_back(roots[i]);
-      out_parts.push_back(P > 1 ? (q | (P << 16)) : 0);
+      out_parts.push_back((P > 1 ? (q | (P << 16)) : 0) | eager);
     }
   }
   roots.swap(out_roots);

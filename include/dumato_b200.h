@@ -83,7 +83,13 @@ typedef struct dm_graph_info {
 /* Engine options. Zero-initialise and set struct_size = sizeof(dm_opts). */
 #define DM_MODE_AUTO 0
 #define DM_MODE_LIST 1     /* sorted-list intersection with warp ballot compaction */
-#define DM_MODE_BITMAP 2   /* per-root local adjacency bitmaps */
+#define DM_MODE_BITMAP 2   /* per-root local adjacency bitmaps, from the graph's clique index when it fits */
+#define DM_MODE_REBUILD 3  /* per-root local adjacency bitmaps rebuilt from the CSR in every launch */
+
+/* How a counting launch moves a root's bitmap block from the clique index into shared memory. */
+#define DM_STAGE_AUTO 0    /* the library's default (bulk asynchronous copies) */
+#define DM_STAGE_LOADS 1   /* 16-byte loads by every lane */
+#define DM_STAGE_TMA 2     /* one bulk asynchronous copy (cp.async.bulk) per block */
 
 #define DM_SCHED_PLAIN 0   /* roots in descending degree order + device donation */
 #define DM_SCHED_LEARNED 1 /* roots ordered by the work predictor (needs a trained predictor) */
@@ -108,7 +114,7 @@ typedef struct dm_opts {
   uint64_t* subtree_counts;    /* optional, n_vertices entries (original ids), overwritten: the
                                   subgraphs counted under each root task (the subtree-size log) */
   int32_t test_flags;          /* DM_TEST_* (tests of the failure paths only), else 0 */
-  int32_t reserved;
+  int32_t staging;             /* DM_STAGE_* (cliques on the index) */
 } dm_opts;
 
 /* test_flags: every warp that finishes waits on a device word nothing sets, so the bounded

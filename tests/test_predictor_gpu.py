@@ -124,3 +124,30 @@ def test_learned_schedule_is_exact(dm, orc, gpu, k):
     a, _ = dm.count_motifs(g, 3, d)
     b, _ = dm.count_motifs(g, 3, d, dm.Options(scheduler=dm.SCHED_LEARNED, predictor=pr.handle))
     assert np.array_equal(a, b)
+
+
+def test_learned_schedule_on_device_every_path(dm, orc, gpu):
+    """The device schedule (inference, bucketed longest-first order, splits, eager-donation
+    flags) is exact on every clique path, on shards, and for motifs; every learned call
+    pays its own scheduling (reported in prep_ms)."""
+    from dumato_b200 import workloads
+
+    Xtr, Ttr = _dataset(dm, "rmat100k", [3], [4, 5, 6])
+    pr = dm.Predictor(seed=4)
+    pr.train(Xtr, Ttr, epochs=20, batch=512, lr=3e-3)
+    g = workloads.make("rmat100k", 1)
+    og = orc.OracleGraph.from_pairs(*g.edges())
+    L = dict(scheduler=dm.SCHED_LEARNED, predictor=pr.handle)
+    for k in (4, 6, 7):
+        want = orc.clique_dag_bytes(og, k)[0]
+        for extra in ({}, {"mode": dm.MODE_REBUILD}, {"staging": dm.STAGE_LOADS}, {"mode": dm.MODE_LIST},
+                      {"test_flags": dm.TEST_EAGER_DONATION}):
+            got, st = dm.count_cliques(g, k, dm.Options(**L, **extra))
+            assert got == want, (k, extra)
+            assert st.prep_ms > 0
+        parts = [dm.count_cliques(g, k, dm.Options(**L, rank=r, world_size=3))[0] for r in range(3)]
+        assert sum(parts) == want
+    d = dm.Dictionary.generate(3)
+    a, _ = dm.count_motifs(g, 3, d)
+    shards = [dm.count_motifs(g, 3, d, dm.Options(**L, rank=r, world_size=2))[0] for r in range(2)]
+    assert np.array_equal(a, shards[0] + shards[1])
