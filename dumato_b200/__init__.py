@@ -35,6 +35,7 @@ STATUS_NAMES = {
 GEN_ER, GEN_CHUNG_LU, GEN_RMAT = 0, 1, 2
 MODE_AUTO, MODE_LIST, MODE_BITMAP, MODE_REBUILD = 0, 1, 2, 3
 STAGE_AUTO, STAGE_LOADS, STAGE_TMA = 0, 1, 2
+FLAG_L2_PERSIST = 1
 QUERY_CLIQUE, QUERY_MOTIF = 0, 1
 AUTOTUNE_MODEL, AUTOTUNE_MEASURE = 0, 1
 SCHED_PLAIN, SCHED_LEARNED, SCHED_ID = 0, 1, 2
@@ -65,7 +66,8 @@ class _Opts(ctypes.Structure):
                 ("vwarp", ctypes.c_int32), ("mode", ctypes.c_int32), ("scheduler", ctypes.c_int32),
                 ("rank", ctypes.c_int32), ("world_size", ctypes.c_int32), ("timeout_ms", ctypes.c_int32),
                 ("predictor", ctypes.c_void_p), ("subtree_counts", ctypes.c_void_p),
-                ("test_flags", ctypes.c_int32), ("staging", ctypes.c_int32)]
+                ("test_flags", ctypes.c_int32), ("staging", ctypes.c_int32), ("flags", ctypes.c_int32),
+                ("reserved", ctypes.c_int32)]
 
 
 class _Stats(ctypes.Structure):
@@ -421,6 +423,7 @@ class Options:
     subtree_counts: Optional[np.ndarray] = None   # uint64[n_vertices], filled per root
     test_flags: int = 0
     staging: int = STAGE_AUTO
+    flags: int = 0
 
     def to_c(self) -> _Opts:
         st = None
@@ -433,7 +436,7 @@ class Options:
                      donations_per_warp=self.donations_per_warp, threshold=self.threshold, vwarp=self.vwarp,
                      mode=self.mode, scheduler=self.scheduler, rank=self.rank, world_size=self.world_size,
                      timeout_ms=self.timeout_ms, predictor=self.predictor, subtree_counts=st,
-                     test_flags=self.test_flags, staging=self.staging)
+                     test_flags=self.test_flags, staging=self.staging, flags=self.flags)
 
 
 @dataclass

@@ -598,6 +598,7 @@ int dm_batch_create(const dm_query* queries, int32_t n, const dm_opts* opts, int
       d.cargs.lb.hungry_trigger = d.trigger;
       d.cargs.lb.min_split = 32;
       d.cargs.arena_dcap = d.arena_dcap;
+      d.cargs.list_vwarp = 32;  // the batch arena holds one list stack per warp
       d.cargs.list_threshold = d.list_threshold;
     } else {
       d.mctx.g = a.g;

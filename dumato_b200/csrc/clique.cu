@@ -19,6 +19,7 @@ static CliqueArgs clique_args(const CliqueLaunch& L, LaunchCtx& ctx) {
                 ctx.test_stall, 32, L.nq};
   a.arena = L.arena;
   a.arena_dcap = L.arena_dcap;
+  a.list_vwarp = (L.list_vwarp == 8 || L.list_vwarp == 16) ? L.list_vwarp : 32;
   a.list_threshold = L.list_threshold;
   a.per_root = L.per_root;
   a.parts = L.parts;
@@ -90,19 +91,7 @@ int clique_index_build(const GraphView& g, const int32_t* roots, int n, void* bl
 }
 
 int clique_launch(const CliqueLaunch& L, LaunchCtx& ctx, int* grid) {
-  CliqueArgs a;
-  a.g = L.g;
-  a.roots = L.roots;
-  a.n_roots = L.n_roots;
-  a.lb = LBArgs{L.ctr, reinterpret_cast<QHeader*>(L.queue),
-                reinterpret_cast<QSlot*>(reinterpret_cast<char*>(L.queue) + sizeof(QHeader) * L.nq), L.qcap, 0,
-                L.max_donations, (long long)ctx.donate_after_us * 1000ll, (long long)ctx.timeout_ms * 1000000ll,
-                ctx.test_stall, 32, L.nq};
-  a.arena = L.arena;
-  a.arena_dcap = L.arena_dcap;
-  a.list_threshold = L.list_threshold;
-  a.per_root = L.per_root;
-  a.parts = L.parts;
+  CliqueArgs a = clique_args(L, ctx);
   switch (L.k) {
     case 2: return launch_nw<2>(a, L.nwmax, ctx, grid);
     case 3: return launch_nw<3>(a, L.nwmax, ctx, grid);

@@ -121,8 +121,10 @@ __device__ __forceinline__ int select_bit(const uint64_t* row, int j) {
 // Shared memory of one warp for a launch whose bitmap roots need up to M words per row:
 // rows | L | prefix of out-degrees | prefix of row popcounts | item range | list stack.
 struct WarpLayout {
-  int rows, L, P, E, range, don, busy, hn, heavy, ptr, n, pos, total;
+  int rows, L, P, E, range, don, busy, hn, heavy, n, pos, total;
 };
+
+constexpr int LIST_LEVELS = 16;  // list-path DFS levels kept per group (k <= 12)
 
 __host__ __device__ constexpr WarpLayout warp_layout(int M) {
   WarpLayout w{};
@@ -135,10 +137,9 @@ __host__ __device__ constexpr WarpLayout warp_layout(int M) {
   w.busy = w.don + 4;
   w.hn = w.busy + 4;
   w.heavy = w.hn + 4;  // 32 deferred heavy items
-  w.ptr = (w.heavy + 4 * 32 + 7) / 8 * 8;
-  w.n = w.ptr + 8 * 16;
-  w.pos = w.n + 4 * 16;
-  w.total = (w.pos + 4 * 16 + 15) / 16 * 16;
+  w.n = (w.heavy + 4 * 32 + 7) / 8 * 8;  // list path: set sizes per level, 4 groups x 16 levels
+  w.pos = w.n + 4 * 4 * LIST_LEVELS;       // list path: next member per level
+  w.total = (w.pos + 4 * 4 * LIST_LEVELS + 15) / 16 * 16;
   return w;
 }
 
@@ -148,8 +149,9 @@ struct CliqueArgs {
   int n_roots;
   LBArgs lb;
   const int32_t* parts;         // optional per-root-entry part word (p | P << 16), else null
-  int32_t* arena;               // list path: K * arena_dcap ints per warp
+  int32_t* arena;               // list path: list_groups x K x arena_dcap ints per warp
   int arena_dcap;
+  int list_vwarp;               // list path: lanes per group (8, 16 or 32)
   int list_threshold;           // roots with d > list_threshold take the list path
   unsigned long long* per_root; // optional: k-cliques found under each root (subtree logger)
 };
@@ -373,19 +375,25 @@ __device__ unsigned long long bitmap_task(const CliqueArgs& a, unsigned char* ws
   return cnt;
 }
 
-// List path for one task (warp-cooperative). Returns this lane's share of the count.
-template <int K, int M>
-__device__ unsigned long long list_task(const CliqueArgs& a, unsigned char* wsm, int root, int d, int b, int e,
-                                        int32_t* my_arena) {
+// List path for one task. The warp's lanes form groups of W (the reference's virtual warps,
+// src/DM_WCV/DuMatoGPU.cu:12-37, 8, 16 or 32 lanes): each group takes first-level
+// candidates from the task's shared range and runs their DFS on its own stack and arena
+// slice (warp_arena + group x K x arena_dcap; level l at l x arena_dcap). Returns this
+// lane's share of the count; the whole warp enters and leaves together.
+template <int K, int M, int W>
+__device__ unsigned long long list_task_w(const CliqueArgs& a, unsigned char* wsm, int root, int d, int b, int e,
+                                          int32_t* warp_arena) {
   constexpr WarpLayout LY = warp_layout(M);
   const int lane = lane_id();
+  const int gl = lane & (W - 1), gi = lane / W;
+  const unsigned gmask = dm_gpm::Group<W>::mask();
   unsigned long long* range = reinterpret_cast<unsigned long long*>(wsm + LY.range);
   int* donations_left = reinterpret_cast<int*>(wsm + LY.don);
   int* busy = reinterpret_cast<int*>(wsm + LY.busy);
+  int* sN = reinterpret_cast<int*>(wsm + LY.n) + gi * LIST_LEVELS;
+  int* sPos = reinterpret_cast<int*>(wsm + LY.pos) + gi * LIST_LEVELS;
+  int32_t* my_arena = warp_arena + (size_t)gi * K * a.arena_dcap;
   const long long t_start = global_ns();
-  const int32_t** sPtr = reinterpret_cast<const int32_t**>(wsm + LY.ptr);
-  int* sN = reinterpret_cast<int*>(wsm + LY.n);
-  int* sPos = reinterpret_cast<int*>(wsm + LY.pos);
   const int32_t* L = a.g.adj + __ldg(a.g.row + root);
   int lo, hi;
   task_range(b, e, d, lo, hi);
@@ -396,18 +404,22 @@ __device__ unsigned long long list_task(const CliqueArgs& a, unsigned char* wsm,
   }
   __syncwarp();
   unsigned long long cnt = 0;
+  int spill_b = 0, spill_e = 0;  // group leader: items split off when the queue was full
   while (true) {
-    int it = 0;
-    if (lane == 0) {
-      it = range_take(range);
-      int ob = 0, oe = 0;
-      if (it >= 0 && range_maybe_donate(a.lb, range, root, donations_left, t_start, busy, ob, oe)) {
-        // lane 0 is the only taker here, so the split can be undone
-        const unsigned long long cur = *reinterpret_cast<volatile unsigned long long*>(range);
-        *range = (cur & 0xffffffffull) | ((unsigned long long)(unsigned)oe << 32);
+    int it = -1;
+    if (gl == 0) {
+      if (spill_b < spill_e) {
+        it = spill_b++;
+      } else {
+        it = range_take(range);
+        int ob = 0, oe = 0;
+        if (it >= 0 && range_maybe_donate(a.lb, range, root, donations_left, t_start, busy, ob, oe)) {
+          spill_b = ob;
+          spill_e = oe;
+        }
       }
     }
-    it = __shfl_sync(FULL_MASK, it, 0);
+    it = __shfl_sync(gmask, it, 0, W);
     if (it < 0) break;
     const int c = __ldg(L + it);
     const int32_t* A = L + it + 1;
@@ -416,19 +428,17 @@ __device__ unsigned long long list_task(const CliqueArgs& a, unsigned char* wsm,
     const int32_t* B = a.g.adj + __ldg(a.g.row + c);
     const int nb = __ldg(a.g.deg + c);
     if constexpr (K == 3) {
-      const int s = dm_gpm::intersect_count<32>(A, na, B, nb);
-      if (lane == 0) cnt += (unsigned)s;
+      const int s = dm_gpm::intersect_count<W>(A, na, B, nb);
+      if (gl == 0) cnt += (unsigned)s;
     } else {
-      // C1 = A cap N+(c), written to level 1 of the arena
-      int32_t* out1 = my_arena + a.arena_dcap;
-      const int m = dm_gpm::extend_intersect<32>(A, na, B, nb, out1);
-      __syncwarp();
-      if (lane == 0) {
-        sPtr[1] = out1;
+      // C1 = A cap N+(c), written to level 1 of the group's arena
+      const int m = dm_gpm::extend_intersect<W>(A, na, B, nb, my_arena + a.arena_dcap);
+      __syncwarp(gmask);
+      if (gl == 0) {
         sN[1] = m;
         sPos[1] = 0;
       }
-      __syncwarp();
+      __syncwarp(gmask);
       int lvl = 1;
       while (lvl >= 1) {
         const int pos = sPos[lvl];
@@ -437,10 +447,10 @@ __device__ unsigned long long list_task(const CliqueArgs& a, unsigned char* wsm,
           --lvl;
           continue;
         }
-        const int32_t* P = sPtr[lvl];
+        const int32_t* P = my_arena + (size_t)lvl * a.arena_dcap;
         const int v = P[pos];
-        __syncwarp();
-        if (lane == 0) {
+        __syncwarp(gmask);
+        if (gl == 0) {
           sPos[lvl] = pos + 1;
           if ((pos & 63) == 63) atomicAdd(&a.lb.ctr->progress, 64ull);
         }
@@ -449,25 +459,33 @@ __device__ unsigned long long list_task(const CliqueArgs& a, unsigned char* wsm,
         const int32_t* B2 = a.g.adj + __ldg(a.g.row + v);
         const int nb2 = __ldg(a.g.deg + v);
         if (lvl + 1 == K - 2) {
-          const int s = dm_gpm::intersect_count<32>(A2, na2, B2, nb2);
-          if (lane == 0) cnt += (unsigned)s;
+          const int s = dm_gpm::intersect_count<W>(A2, na2, B2, nb2);
+          if (gl == 0) cnt += (unsigned)s;
         } else {
-          int32_t* out = my_arena + (size_t)(lvl + 1) * a.arena_dcap;
-          const int m2 = dm_gpm::extend_intersect<32>(A2, na2, B2, nb2, out);
-          __syncwarp();
+          const int m2 = dm_gpm::extend_intersect<W>(A2, na2, B2, nb2, my_arena + (size_t)(lvl + 1) * a.arena_dcap);
+          __syncwarp(gmask);
           ++lvl;
-          if (lane == 0) {
-            sPtr[lvl] = out;
+          if (gl == 0) {
             sN[lvl] = m2;
             sPos[lvl] = 0;
           }
         }
-        __syncwarp();
+        __syncwarp(gmask);
       }
     }
   }
   __syncwarp();
   return cnt;
+}
+
+template <int K, int M>
+__device__ __forceinline__ unsigned long long list_task(const CliqueArgs& a, unsigned char* wsm, int root, int d,
+                                                        int b, int e, int32_t* warp_arena) {
+  switch (a.list_vwarp) {
+    case 8: return list_task_w<K, M, 8>(a, wsm, root, d, b, e, warp_arena);
+    case 16: return list_task_w<K, M, 16>(a, wsm, root, d, b, e, warp_arena);
+    default: return list_task_w<K, M, 32>(a, wsm, root, d, b, e, warp_arena);
+  }
 }
 
 // One root task: items [b, e) of root (task_range encoding), on the bitmap path when the

@@ -269,7 +269,6 @@ __device__ unsigned long long heavy_run(const CachedArgs& a, const TaskWords& tw
   const long long t_start = global_ns();
   const int path[1] = {it};
   unsigned long long cnt = 0;
-  unsigned taken = 0;
   int j;
   while ((j = range_take(tw.range)) >= 0) {
     const int c3 = select_bits<NW>(S, j);
@@ -280,7 +279,8 @@ __device__ unsigned long long heavy_run(const CachedArgs& a, const TaskWords& tw
 #pragma unroll
     for (int w = 0; w < NW; ++w) T.w[w] = (w < w3 ? 0ull : (w == w3 ? (S.w[w] & above) : S.w[w])) & rc[w];
     if (popc(T) >= K - 4) cnt += count_rec_hb<(K >= 6 ? K - 5 : 0), NW>(T, rows, &a.c.lb.ctr->progress);
-    if ((++taken & 3) == 0) {
+    // every position is a whole subtree below level 2: check for hungry warps after each
+    {
       int ob = 0, oe = 0;
       if (range_maybe_donate(a.c.lb, tw.range, root, tw.don, t_start, tw.busy, ob, oe, p, 2, 1, path, eager)) {
         for (int q = ob; q < oe; ++q) {
@@ -459,7 +459,8 @@ __global__ void __launch_bounds__(256) clique_cached_kernel(const __grid_constan
   unsigned phase = 0;
   const int gw = blockIdx.x * (blockDim.x >> 5) + warp_in_block();
   const int total_warps = gridDim.x * (blockDim.x >> 5);
-  int32_t* my_arena = a.c.arena ? a.c.arena + (size_t)gw * K * a.c.arena_dcap : nullptr;
+  int32_t* my_arena =
+      a.c.arena ? a.c.arena + (size_t)gw * (32 / a.c.list_vwarp) * K * a.c.arena_dcap : nullptr;
   unsigned long long cnt = 0, ntasks = 0;
   int unflushed = 0;  // lane 0: finished chunk entries not yet subtracted from pending
   bool first_claim = true;

@@ -21,7 +21,7 @@ __global__ void __launch_bounds__(256) clique_kernel(const __grid_constant__ Cli
   unsigned char* wsm = smem + (size_t)LY.total * warp_in_block();
   const size_t gw = (size_t)blockIdx.x * (blockDim.x >> 5) + warp_in_block();
   const int total_warps = gridDim.x * (blockDim.x >> 5);
-  int32_t* my_arena = a.arena ? a.arena + gw * (size_t)K * a.arena_dcap : nullptr;
+  int32_t* my_arena = a.arena ? a.arena + gw * (size_t)(32 / a.list_vwarp) * K * a.arena_dcap : nullptr;
   unsigned long long cnt = 0, ntasks = 0;
   while (true) {
     int first = 0, count = 0, b = 0, e = -1, ok = 0;

@@ -161,6 +161,52 @@ int select_device(const dm_opts* o, LaunchCtx& ctx) {
   return DM_OK;
 }
 
+// Access-policy window for one call (DM_FLAG_L2_PERSIST): the hottest device array of the
+// call (the clique index, else the adjacency) is marked persisting on the call's stream, with
+// the context's persisting set-aside raised to cover it. Everything is put back when the
+// guard goes out of scope, after the call's stream has been synchronised: the window is
+// removed, persisting lines return to normal, and the previous set-aside is restored.
+struct L2Window {
+  bool active = false;
+  size_t prev_limit = 0;
+  cudaStream_t st = nullptr;
+  size_t window_bytes = 0;
+
+  int begin(int dev, cudaStream_t stream, const void* base, size_t bytes) {
+    int max_persist = 0, max_window = 0;
+    DM_CUDA(cudaDeviceGetAttribute(&max_persist, cudaDevAttrMaxPersistingL2CacheSize, dev));
+    DM_CUDA(cudaDeviceGetAttribute(&max_window, cudaDevAttrMaxAccessPolicyWindowSize, dev));
+    if (max_persist <= 0 || max_window <= 0 || !base || bytes == 0) return DM_OK;
+    DM_CUDA(cudaDeviceGetLimit(&prev_limit, cudaLimitPersistingL2CacheSize));
+    const size_t want = std::min(bytes, (size_t)max_persist);
+    DM_CUDA(cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, want));
+    active = true;
+    st = stream;
+    cudaStreamAttrValue v{};
+    v.accessPolicyWindow.base_ptr = const_cast<void*>(base);
+    v.accessPolicyWindow.num_bytes = std::min(bytes, (size_t)max_window);
+    v.accessPolicyWindow.hitRatio = std::min(1.0f, (float)want / (float)v.accessPolicyWindow.num_bytes);
+    v.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
+    v.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
+    window_bytes = v.accessPolicyWindow.num_bytes;
+    DM_CUDA(cudaStreamSetAttribute(stream, cudaStreamAttributeAccessPolicyWindow, &v));
+    return DM_OK;
+  }
+
+  ~L2Window() {
+    if (!active) return;
+    cudaStreamAttrValue v{};
+    v.accessPolicyWindow.num_bytes = 0;
+    v.accessPolicyWindow.hitRatio = 0.f;
+    v.accessPolicyWindow.hitProp = cudaAccessPropertyNormal;
+    v.accessPolicyWindow.missProp = cudaAccessPropertyNormal;
+    cudaStreamSetAttribute(st, cudaStreamAttributeAccessPolicyWindow, &v);
+    cudaCtxResetPersistingL2Cache();
+    cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, prev_limit);
+    cudaGetLastError();
+  }
+};
+
 // Workspaces of released graphs, per device, handed to the next graph that needs one on that
 // device. A graph's own device memory is its CSR copies and root orders; the scratch, the
 // donation queue, the counters and the events are not tied to a graph, and allocating and
@@ -353,6 +399,7 @@ int check_opts(const dm_opts* o) {
     return fail(DM_EINVAL, "dm_opts.struct_size does not match this library");
   if (o->mode < 0 || o->mode > 3) return fail(DM_EINVAL, "dm_opts.mode out of range");
   if (o->staging < 0 || o->staging > 2) return fail(DM_EINVAL, "dm_opts.staging out of range");
+  if (o->flags & ~DM_FLAG_L2_PERSIST) return fail(DM_EINVAL, "dm_opts.flags has unknown bits");
   if (o->scheduler < 0 || o->scheduler > 2) return fail(DM_EINVAL, "dm_opts.scheduler out of range");
   if (o->vwarp != 0 && o->vwarp != 8 && o->vwarp != 16 && o->vwarp != 32)
     return fail(DM_EINVAL, "dm_opts.vwarp must be 0, 8, 16 or 32");
@@ -680,9 +727,11 @@ int dm_count_cliques(dm_graph* g, int32_t k, const dm_opts* o, uint64_t* count, 
                               ctx.stream));
     d_roots = ws.d_tasks;
   }
+  // list path: virtual-warp groups of 8, 16 or 32 lanes (32 unless dm_opts.vwarp says otherwise)
+  L.list_vwarp = (ctx.vwarp == 8 || ctx.vwarp == 16) ? ctx.vwarp : 32;
   if (need_arena) {
     L.arena_dcap = max_d + 4;
-    const size_t per_warp = (size_t)k * L.arena_dcap * sizeof(int32_t);
+    const size_t per_warp = (size_t)(32 / L.list_vwarp) * k * L.arena_dcap * sizeof(int32_t);
     const size_t budget = (size_t)8 << 30;
     ctx.arena_warps = (int)std::min<size_t>((size_t)clique_max_warps(ctx.num_sms), std::max<size_t>(8, budget / per_warp));
     if ((rc = ensure_ws_bytes(&ws.d_scratch, &ws.scratch_cap, per_warp * ctx.arena_warps))) return rc;
@@ -721,6 +770,12 @@ int dm_count_cliques(dm_graph* g, int32_t k, const dm_opts* o, uint64_t* count, 
     }
   }
   if ((rc = init_counters(ws, n_roots, ctx.stream, cursor))) return rc;
+  L2Window l2;
+  if (o && (o->flags & DM_FLAG_L2_PERSIST)) {
+    if (use_index) rc = l2.begin(ctx.device, ctx.stream, s->d_blocks, s->index_bytes);
+    else rc = l2.begin(ctx.device, ctx.stream, s->dg.d_oadj, sizeof(int32_t) * g->pad_adj[1].size());
+    if (rc) return rc;
+  }
   DM_CUDA(cudaEventRecord(ws.k0, ctx.stream));
   if (n_roots > 0) {
     rc = use_index ? clique_cached_launch(L, ctx, grid) : clique_launch(L, ctx, &grid);
@@ -756,7 +811,7 @@ int dm_count_cliques(dm_graph* g, int32_t k, const dm_opts* o, uint64_t* count, 
     st->idle_polls = h.idle_polls;
     st->nodes = h.nodes;
     st->mode_used = mode == DM_MODE_LIST ? DM_MODE_LIST : (use_index ? DM_MODE_BITMAP : DM_MODE_REBUILD);
-    st->vwarp_used = 32;
+    st->vwarp_used = L.list_vwarp;
     st->grid = grid;
     st->block = 256;
     st->kernel_launches = ctx.launches;
@@ -917,6 +972,10 @@ int dm_count_motifs(dm_graph* g, int32_t k, const dm_dictionary* dict, const dm_
   L.vwarp = vwarp;
   L.bits = d_bits;
   L.bit_words = bit_words;
+  L2Window l2;
+  if (o && (o->flags & DM_FLAG_L2_PERSIST) &&
+      (rc = l2.begin(ctx.device, ctx.stream, s->dg.d_adj, sizeof(int32_t) * g->pad_adj[0].size())))
+    return rc;
   DM_CUDA(cudaEventRecord(ws.k0, ctx.stream));
   int grid = 0;
   if (n_roots > 0) {

@@ -128,8 +128,9 @@ struct CliqueLaunch {
   int qcap = 0;                  // slots per shard
   int nq = 1;                    // shards
   int max_donations = 16;        // per task
-  int32_t* arena = nullptr;      // list path
+  int32_t* arena = nullptr;      // list path: (32 / list_vwarp) x k x arena_dcap ints per warp
   int arena_dcap = 0;
+  int list_vwarp = 32;           // list path: lanes per group (8, 16 or 32)
   int list_threshold = 256;
   int nwmax = 1;
   unsigned long long* per_root = nullptr;

@@ -21,7 +21,12 @@ struct MotifArgs {
   int2* arena;                 // per warp: 32/W group arenas of c.arena_stride int2
   uint32_t* bits;              // per warp: 32/W groups x 2 membership bitmaps of c.bit_words (or null)
   const int32_t* parts;        // optional per-root-entry part word (p | P << 16)
+  int bits_smem;               // the bitmaps live in shared memory (zeroed at launch), not in `bits`
 };
+
+// Shared-memory budget of one block's membership bitmaps; larger graphs keep them in global
+// memory.
+constexpr size_t MOTIF_SMEM_BITS_MAX = 64 * 1024;
 
 template <int K, int W>
 __global__ void __launch_bounds__(32 * MOTIF_WARPS, 4) motif_kernel(const __grid_constant__ MotifArgs a) {
@@ -32,13 +37,18 @@ __global__ void __launch_bounds__(32 * MOTIF_WARPS, 4) motif_kernel(const __grid
   const int wib = warp_in_block();
   MotifShared* ws = reinterpret_cast<MotifShared*>(wbase + motif_warp_smem<W>() * wib);
   MotifGroup* groups = reinterpret_cast<MotifGroup*>(ws + 1);
-  for (int cl = threadIdx.x; cl < a.n_classes; cl += blockDim.x) bhist[cl] = 0;
-  __syncthreads();
   const MotifCtx& c = a.c;
+  const size_t warp_bit_words = (size_t)c.bit_words * 2 * (32 / W);
+  uint32_t* sbits = reinterpret_cast<uint32_t*>(wbase + motif_warp_smem<W>() * MOTIF_WARPS);
+  for (int cl = threadIdx.x; cl < a.n_classes; cl += blockDim.x) bhist[cl] = 0;
+  if (a.bits_smem)
+    for (size_t i = threadIdx.x; i < warp_bit_words * MOTIF_WARPS; i += blockDim.x) sbits[i] = 0u;
+  __syncthreads();
   const size_t gw = (size_t)blockIdx.x * MOTIF_WARPS + wib;
   const int total_warps = gridDim.x * MOTIF_WARPS;
   int2* warp_arena = a.arena + gw * (size_t)c.arena_stride * (32 / W);
-  uint32_t* warp_bits = a.bits ? a.bits + gw * (size_t)c.bit_words * 2 * (32 / W) : nullptr;
+  uint32_t* warp_bits = a.bits_smem ? sbits + wib * warp_bit_words
+                                    : (a.bits ? a.bits + gw * warp_bit_words : nullptr);
   unsigned long long ntasks = 0, nodes = 0;
   while (true) {
     int first = 0, count = 0, b = 0, e = -1, ok = 0, level = 0;
@@ -92,8 +102,10 @@ size_t motif_arena_stride(int k, int maxdeg, int vwarp) {
 template <int K, int W>
 static int launch_motif(MotifArgs a, LaunchCtx& ctx, int* grid_out) {
   const int block = 32 * MOTIF_WARPS;
-  const size_t smem =
-      sizeof(unsigned long long) * ((a.n_classes + 1) & ~1) + motif_warp_smem<W>() * MOTIF_WARPS;
+  const size_t bits_bytes = (size_t)a.c.bit_words * 2 * (32 / W) * sizeof(uint32_t) * MOTIF_WARPS;
+  a.bits_smem = a.bits && a.c.bit_words > 0 && bits_bytes <= MOTIF_SMEM_BITS_MAX ? 1 : 0;
+  const size_t smem = sizeof(unsigned long long) * ((a.n_classes + 1) & ~1) +
+                      motif_warp_smem<W>() * MOTIF_WARPS + (a.bits_smem ? bits_bytes : 0);
   auto kern = motif_kernel<K, W>;
   DM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int occ = 0;
@@ -140,6 +152,7 @@ int motif_launch(const MotifLaunch& L, LaunchCtx& ctx, int* grid) {
   a.hist = L.hist;
   a.arena = reinterpret_cast<int2*>(L.arena);
   a.parts = L.parts;
+  a.bits_smem = 0;
   const int w = (L.vwarp == 8 || L.vwarp == 16) ? L.vwarp : 32;
   switch (L.k) {
     case 3: return launch_motif_w<3>(a, w, ctx, grid);

@@ -32,7 +32,7 @@
 extern "C" {
 #endif
 
-#define DM_ABI_VERSION 1
+#define DM_ABI_VERSION 2
 
 #if defined(__GNUC__)
 #define DM_API __attribute__((visibility("default")))
@@ -104,7 +104,10 @@ typedef struct dm_opts {
   int32_t donations_per_warp;  /* reference argv[5]: donations one task may make (0 = 64) */
   int32_t threshold;           /* reference argv[6]: idle-warp percentage that triggers donation;
                                   >= 100 disables donation (clique_PA.cu:78) */
-  int32_t vwarp;               /* virtual-warp width 0 (auto), 8, 16 or 32 */
+  int32_t vwarp;               /* virtual-warp width 0 (auto), 8, 16 or 32: motifs, the lanes sharing
+                                  a task's second vertices per group; cliques, the lanes running one
+                                  first-level candidate's DFS on the list path (the bitmap paths run
+                                  one DFS per lane) */
   int32_t mode;                /* DM_MODE_* */
   int32_t scheduler;           /* DM_SCHED_* */
   int32_t rank;                /* root shard: this process counts roots r with r % world == rank */
@@ -115,7 +118,15 @@ typedef struct dm_opts {
                                   subgraphs counted under each root task (the subtree-size log) */
   int32_t test_flags;          /* DM_TEST_* (tests of the failure paths only), else 0 */
   int32_t staging;             /* DM_STAGE_* (cliques on the index) */
+  int32_t flags;               /* DM_FLAG_* */
+  int32_t reserved;
 } dm_opts;
+
+/* flags: for the duration of the call, mark the graph's device CSR (and the clique index) as
+   persisting in L2 through an access-policy window on the call's stream, with the context's
+   persisting set-aside raised to cover it; the window, the set-aside and the persisting lines
+   are reset before the call returns. */
+#define DM_FLAG_L2_PERSIST 1
 
 /* test_flags: every warp that finishes waits on a device word nothing sets, so the bounded
    wait expires and the call returns DM_ETIMEOUT (exercises the timeout path without a

@@ -3,6 +3,7 @@ k = 3..6): quick -> cg_local (int32) and cg_local -> cg_global (uint64). Run whe
 DuMato sources are available:
 
     python tests/golden/make_dictionary_fixtures.py /path/to/DuMato
+    DUMATO_REF_ROOT=/path/to/DuMato python tests/golden/make_dictionary_fixtures.py
 """
 from __future__ import annotations
 
@@ -38,4 +39,9 @@ def main(root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    import os
+
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("DUMATO_REF_ROOT")
+    if not root:
+        sys.exit("usage: make_dictionary_fixtures.py /path/to/DuMato (or set DUMATO_REF_ROOT)")
+    main(root)

@@ -49,4 +49,4 @@ def test_bad_arguments(dm):
             assert e.status in (-1, -5)
         else:
             raise AssertionError
-    assert dm.lib().dm_abi_version() == 1
+    assert dm.lib().dm_abi_version() == 2

@@ -128,3 +128,19 @@ def test_donations_happen_and_stay_exact(dm, orc, gpu):
     assert st.donations > 0
     off, _ = dm.count_cliques(g, 5, dm.Options(threshold=100))
     assert off == want
+
+
+@pytest.mark.parametrize("vwarp", [8, 16, 32])
+def test_list_path_virtual_warps(dm, orc, gpu, vwarp):
+    """The list path with groups of 8, 16 or 32 lanes per first-level candidate (the
+    reference's DM_WCV clique variant) gives the oracle's counts, with donations on."""
+    from dumato_b200 import workloads
+
+    for g in (dm.Graph.load_edgelist(GOLDEN / "citeseer.edgelist"), workloads.make("rmat100k", 1)):
+        og = _oracle_graph(orc, g)
+        for k in (3, 4, 5, 6):
+            want = orc.clique_dag_bytes(og, k)[0]
+            got, st = dm.count_cliques(g, k, dm.Options(mode=dm.MODE_LIST, vwarp=vwarp,
+                                                        test_flags=dm.TEST_EAGER_DONATION))
+            assert got == want, (vwarp, k)
+            assert st.vwarp_used == vwarp
