@@ -97,6 +97,8 @@ _SIGNATURES = {
     "dm_last_error": (ctypes.c_char_p, []),
     "dm_device_count": (ctypes.c_int, []),
     "dm_graph_load_edgelist": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(_P)]),
+    "dm_graph_load_edgelist_device": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(_Opts), ctypes.POINTER(_P),
+                                                     ctypes.POINTER(ctypes.c_double)]),
     "dm_graph_from_edges": (ctypes.c_int, [_P, _P, ctypes.c_int64, ctypes.c_int32, ctypes.POINTER(_P)]),
     "dm_graph_generate": (ctypes.c_int, [ctypes.POINTER(_GenParams), ctypes.POINTER(_P)]),
     "dm_graph_info_get": (ctypes.c_int, [_P, ctypes.POINTER(_GraphInfo)]),
@@ -113,6 +115,7 @@ _SIGNATURES = {
     "dm_dictionary_connected": (ctypes.c_int, [_P, _P]),
     "dm_dictionary_free": (None, [_P]),
     "dm_clique_work_model": (ctypes.c_int, [_P, ctypes.c_int32, _P, _P]),
+    "dm_motif_work_model": (ctypes.c_int, [_P, ctypes.c_int32, _P, _P]),
     "dm_plan_roots": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(_Opts), _P, _P, ctypes.c_int64,
                                      ctypes.POINTER(ctypes.c_int64)]),
     "dm_predictor_create": (ctypes.c_int, [ctypes.c_uint64, ctypes.POINTER(_P)]),
@@ -194,6 +197,17 @@ class Graph:
         h = _P()
         _check(lib().dm_graph_load_edgelist(str(path).encode(), ctypes.byref(h)))
         return cls(h)
+
+    @classmethod
+    def load_edgelist_device(cls, path: str | os.PathLike, opts: "Optional[Options]" = None) -> "tuple[Graph, float]":
+        """The edgelist reader on the GPU (parse, dedup, symmetrise, orient on the device);
+        returns the graph and the device time in ms."""
+        h = _P()
+        ms = ctypes.c_double()
+        o = (opts or Options()).to_c()
+        _check(lib().dm_graph_load_edgelist_device(str(path).encode(), ctypes.byref(o), ctypes.byref(h),
+                                                   ctypes.byref(ms)))
+        return cls(h), ms.value
 
     @classmethod
     def from_edges(cls, src: Sequence[int], dst: Sequence[int], n_vertices: int = 0) -> "Graph":
@@ -462,6 +476,15 @@ class Stats:
         return cls(s.kernel_ms, s.prep_ms, s.tasks, s.donations, s.idle_polls, s.nodes, s.mode_used,
                    s.vwarp_used, s.grid, s.block, s.kernel_launches, s.idle_warp_fraction, s.max_task_ms,
                    s.max_task_root, s.prefix_donations)
+
+
+def motif_work_model(g: Graph, k: int) -> tuple[int, int]:
+    """(DFS prefixes, algorithmic bytes) of k-motif counting on g: the byte model behind the
+    motif roofline figures (host-side accounting, not a counting path)."""
+    n = ctypes.c_uint64()
+    b = ctypes.c_uint64()
+    _check(lib().dm_motif_work_model(g.handle, int(k), ctypes.byref(n), ctypes.byref(b)))
+    return n.value, b.value
 
 
 def clique_work_model(g: Graph, k: int) -> tuple[int, int]:

@@ -7,6 +7,8 @@
 // self-loops in its adjacency sets; they never take part in a count there (every
 // extension is filtered by "> v"), so they are dropped here and only counted.
 #include <algorithm>
+#include <atomic>
+#include <thread>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -499,6 +501,112 @@ int dm_clique_work_model(dm_graph* g, int32_t k, uint64_t* nodes_out, uint64_t* 
       nC[l] = m;
       pos[l] = 0;
     }
+  }
+  *nodes_out = nodes;
+  *bytes_out = bytes;
+  return DM_OK;
+}
+
+// Work model of the motif path (host-side accounting for the roofline; it counts nothing):
+// the DFS of the reference's motif driver visits, below every root v0, the canonical
+// prefixes (v_0..v_t), t <= k-2, whose extension step reads the adjacency rows of the
+// prefix and writes the deduplicated union above v0 with its sources (extend(0,k),
+// DuMatoGPU.cu:1702-1721): 4 sum_i deg(v_i) + 8 |union| bytes; each leaf candidate of the
+// last level costs 4(k-1) + 8 (its adjacency probes and the dictionary read,
+// aggregate_pattern 930-967). Only internal prefixes are walked: with U_t the union and
+// E_t the valid extensions, taking w from E_t gives excl(w) = N(w) above v0 outside U_t,
+// U_{t+1} = U_t + excl(w) and E_{t+1} = {e in E_t : e > w} + excl(w), and the leaves of a
+// last-level prefix are |E_{k-2}|.
+namespace {
+
+struct MotifModel {
+  const dm_graph* g;
+  int k;
+  std::vector<int32_t> mark;     // 1 + depth at which a vertex joined U (0 = not in U)
+  std::vector<int32_t> ebuf;     // E_t per level
+  std::vector<int32_t> xbuf;     // excl per level
+  size_t cap;
+  uint64_t nodes = 0, bytes = 0;
+
+  int32_t deg(int32_t v) const { return (int32_t)(g->row[v + 1] - g->row[v]); }
+
+  void visit(int32_t v0, int t, const int32_t* E, int32_t nE, uint64_t degsum, uint64_t usize) {
+    ++nodes;
+    bytes += 4 * degsum + 8 * usize;
+    if (t == k - 2) {
+      bytes += (uint64_t)nE * (4ull * (uint64_t)(k - 1) + 8ull);
+      return;
+    }
+    int32_t* X = xbuf.data() + (size_t)(t + 1) * cap;
+    int32_t* En = ebuf.data() + (size_t)(t + 1) * cap;
+    for (int32_t i = 0; i < nE; ++i) {
+      const int32_t w = E[i];
+      int32_t nx = 0;
+      for (int64_t e = g->row[w]; e < g->row[w + 1]; ++e) {
+        const int32_t x = g->adj[e];
+        if (x > v0 && mark[x] == 0) {
+          mark[x] = t + 2;
+          X[nx++] = x;
+        }
+      }
+      // E_{t+1}: members of E_t above w, then excl(w), merged in id order
+      std::sort(X, X + nx);
+      int32_t m = 0, a = 0, b = 0;
+      const int32_t* S = E + i + 1;  // E_t is id-sorted: the members above w are its suffix
+      const int32_t ns = nE - i - 1;
+      while (a < ns || b < nx) {
+        if (b >= nx || (a < ns && S[a] < X[b])) En[m++] = S[a++];
+        else En[m++] = X[b++];
+      }
+      visit(v0, t + 1, En, m, degsum + (uint64_t)deg(w), usize + (uint64_t)nx);
+      for (int32_t j = 0; j < nx; ++j) mark[X[j]] = 0;
+    }
+  }
+};
+
+}  // namespace
+
+int dm_motif_work_model(dm_graph* g, int32_t k, uint64_t* nodes_out, uint64_t* bytes_out) {
+  if (!g || !nodes_out || !bytes_out) return fail(DM_EINVAL, "dm_motif_work_model: null argument");
+  if (k < 3 || k > 7) return fail(DM_EINVAL, "dm_motif_work_model: k must be in [3, 7]");
+  const int32_t n = g->n;
+  const unsigned nt = std::max(1u, std::min(64u, std::thread::hardware_concurrency()));
+  std::vector<uint64_t> tn(nt, 0), tb(nt, 0);
+  std::atomic<int32_t> next{0};
+  auto work = [&](unsigned id) {
+    MotifModel M;
+    M.g = g;
+    M.k = k;
+    M.mark.assign((size_t)std::max(n, 1), 0);
+    M.cap = (size_t)g->max_degree * (size_t)(k - 1) + 1;
+    M.ebuf.assign(M.cap * (size_t)k, 0);
+    M.xbuf.assign(M.cap * (size_t)k, 0);
+    while (true) {
+      const int32_t v0 = next.fetch_add(1);
+      if (v0 >= n) break;
+      int32_t* E0 = M.ebuf.data();
+      int32_t n0 = 0;
+      for (int64_t e = g->row[v0]; e < g->row[v0 + 1]; ++e) {
+        const int32_t x = g->adj[e];
+        if (x > v0) {
+          E0[n0++] = x;
+          M.mark[x] = 1;
+        }
+      }
+      M.visit(v0, 0, E0, n0, (uint64_t)M.deg(v0), (uint64_t)n0);
+      for (int32_t j = 0; j < n0; ++j) M.mark[E0[j]] = 0;
+    }
+    tn[id] = M.nodes;
+    tb[id] = M.bytes;
+  };
+  std::vector<std::thread> th;
+  for (unsigned i = 1; i < nt; ++i) th.emplace_back(work, i);
+  work(0);
+  for (auto& t : th) t.join();
+  uint64_t nodes = 0, bytes = 0;
+  for (unsigned i = 0; i < nt; ++i) {
+    nodes += tn[i];
+    bytes += tb[i];
   }
   *nodes_out = nodes;
   *bytes_out = bytes;

@@ -161,6 +161,13 @@ DM_API int dm_device_count(void);
 
 /* ---- graphs ---- */
 DM_API int dm_graph_load_edgelist(const char* path, dm_graph** out);
+/* The same reader on the GPU (replaces Graph::Graph + the CSR build, src/main/Graph.cpp:17-75,
+   src/main/DuMatoCPU.cu:94-108): the file's bytes are parsed, deduplicated, symmetrised
+   and degree-oriented on the device of opts (may be NULL), and the graph is identical to
+   dm_graph_load_edgelist's (same CSR, orientation, counts and format errors). Files below
+   2 GiB. *device_ms (may be NULL) receives the device time from the byte upload to the
+   read-back of the CSRs. */
+DM_API int dm_graph_load_edgelist_device(const char* path, const dm_opts* opts, dm_graph** out, double* device_ms);
 DM_API int dm_graph_from_edges(const int32_t* src, const int32_t* dst, int64_t n_pairs,
                         int32_t n_vertices, dm_graph** out);
 DM_API int dm_graph_generate(const dm_gen_params* params, dm_graph** out);
@@ -243,6 +250,13 @@ DM_API void dm_batch_free(dm_batch* b);
    a candidate set C_child = C_parent cap N+(v) costs 4(|C_parent| + |N+(v)|) + 4|C_child|
    bytes (level 0: 4|N+(v0)| + 4|C_0|). Writes the node count and the byte total. */
 DM_API int dm_clique_work_model(dm_graph* g, int32_t k, uint64_t* nodes, uint64_t* bytes);
+
+/* Work model of the motif path (host-side, for roofline accounting only; it counts nothing):
+   every canonical prefix (v_0..v_t), t <= k-2, of the reference's motif DFS costs
+   4 sum_i deg(v_i) + 8 |union of their neighbourhoods above v_0| bytes (extend(0,k)), and
+   every leaf candidate 4(k-1) + 8 (adjacency probes and the dictionary read). Writes the
+   number of prefixes and the byte total; walks the prefixes only (not the leaves). */
+DM_API int dm_motif_work_model(dm_graph* g, int32_t k, uint64_t* nodes, uint64_t* bytes);
 
 /* k-cliques of a DAG already in device memory, with no GPU allocation (no counterpart in
    the reference). For callers that cannot call cudaMalloc: code that runs inside another

@@ -86,3 +86,21 @@ def test_generator_argument_errors(dm):
         dm.Graph.generate(dm.GEN_ER, 10, 100, seed=1)
     with pytest.raises(dm.DMError):
         dm.Graph.generate(7, 10, 10, seed=1)
+
+
+@pytest.mark.parametrize("k", [3, 4, 5])
+def test_motif_work_model_matches_oracle_bytes(dm, orc, k):
+    """The host work model walks only the internal prefixes, yet its byte total equals the
+    oracle's, which charges every extension and leaf while enumerating."""
+    rng = np.random.default_rng(40 + k)
+    graphs = [dm.Graph.load_edgelist(GOLDEN / "citeseer.edgelist")] if k < 5 else []
+    for _ in range(3):
+        n = int(rng.integers(30, 90))
+        s, t = rng.integers(0, n, 4 * n), rng.integers(0, n, 4 * n)
+        graphs.append(dm.Graph.from_edges(s, t))
+    for g in graphs:
+        og = orc.OracleGraph.from_pairs(*g.edges())
+        d = dm.Dictionary.generate(k)
+        q2c, _ = d.tables()
+        _, want = orc.motifs(og, k, q2c, d.n_classes, with_bytes=True)
+        assert dm.motif_work_model(g, k)[1] == want
