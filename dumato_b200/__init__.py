@@ -59,6 +59,15 @@ class _GraphInfo(ctypes.Structure):
                 ("n_input_pairs", ctypes.c_int64)]
 
 
+class _Report(ctypes.Structure):
+    _fields_ = [("elapsed_ms", ctypes.c_double), ("warps", ctypes.c_int32), ("hungry_warps", ctypes.c_int32),
+                ("roots_claimed", ctypes.c_int64), ("roots_total", ctypes.c_int64), ("pending", ctypes.c_int64),
+                ("donations", ctypes.c_uint64), ("progress", ctypes.c_uint64)]
+
+
+_REPORT_FN = ctypes.CFUNCTYPE(None, ctypes.POINTER(_Report), ctypes.c_void_p)
+
+
 class _Opts(ctypes.Structure):
     _fields_ = [("struct_size", ctypes.c_int32), ("device", ctypes.c_int32), ("stream", ctypes.c_uint64),
                 ("threads", ctypes.c_int32), ("block_size", ctypes.c_int32),
@@ -67,7 +76,7 @@ class _Opts(ctypes.Structure):
                 ("rank", ctypes.c_int32), ("world_size", ctypes.c_int32), ("timeout_ms", ctypes.c_int32),
                 ("predictor", ctypes.c_void_p), ("subtree_counts", ctypes.c_void_p),
                 ("test_flags", ctypes.c_int32), ("staging", ctypes.c_int32), ("flags", ctypes.c_int32),
-                ("reserved", ctypes.c_int32)]
+                ("report_ms", ctypes.c_int32), ("report", _REPORT_FN), ("report_user", ctypes.c_void_p)]
 
 
 class _Stats(ctypes.Structure):
@@ -438,6 +447,8 @@ class Options:
     test_flags: int = 0
     staging: int = STAGE_AUTO
     flags: int = 0
+    report: Optional[object] = None   # callable(dict), called every report_ms while a kernel runs
+    report_ms: int = 0
 
     def to_c(self) -> _Opts:
         st = None
@@ -450,7 +461,23 @@ class Options:
                      donations_per_warp=self.donations_per_warp, threshold=self.threshold, vwarp=self.vwarp,
                      mode=self.mode, scheduler=self.scheduler, rank=self.rank, world_size=self.world_size,
                      timeout_ms=self.timeout_ms, predictor=self.predictor, subtree_counts=st,
-                     test_flags=self.test_flags, staging=self.staging, flags=self.flags)
+                     test_flags=self.test_flags, staging=self.staging, flags=self.flags,
+                     report_ms=self.report_ms if self.report else 0, report=self._report_fn(),
+                     report_user=None)
+
+    def _report_fn(self):
+        if self.report is None:
+            return _REPORT_FN()
+        user = self.report
+
+        def cb(sample, _user):
+            r = sample.contents
+            user({f: getattr(r, f) for f, _ in _Report._fields_})
+
+        fn = _REPORT_FN(cb)
+        # the C function pointer must outlive the call: keep it with the options
+        object.__setattr__(self, "_report_keep", fn)
+        return fn
 
 
 @dataclass

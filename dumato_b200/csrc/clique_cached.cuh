@@ -12,11 +12,14 @@
 // (src/main/DuMatoGPU.cu:1194-1220, 1769-1771) as AND + popc over the rows.
 //
 // Task structure (one warp per task):
-//   chunk tasks: a run of consecutive entries of the root list; the warp stages as many of
-//       their blocks as fit in one round of loads, then counts them one after the other.
-//       Warp w's first chunk is assigned statically (no cursor atomics at launch), and the
-//       pending-count decrements of finished roots are deferred until the warp runs out of
-//       work.
+//   chunk tasks: entries of the root list; the warp stages as many of their blocks as fit
+//       in one round of loads, then counts them one after the other. The first CHUNK_MAX x T
+//       entries (T warps) are dealt statically and interleaved - warp w takes w, w + T, ... -
+//       so the heaviest roots of the descending order start on different warps and no cursor
+//       atomics are needed; the rest is claimed from the cursor in runs. Completions of the
+//       static entries are settled once per block, later ones once per warp when it runs out
+//       of work, and the final sums once per block: a launch issues few global atomics on the
+//       shared words.
 //   level-0 donations: (root, item range) as in clique.cuh.
 //   level-1 donations (k >= 6): (root, item, range of positions in the item's candidate
 //       set S = row[c1] & row[c2]): the positions choose the third local vertex c3, so a
@@ -174,8 +177,11 @@ struct CachedArgs {
   const RootDesc* desc;        // task list (c.n_roots entries)
   const uint4* blocks;         // the clique index
   const uint32_t* boff;        // block offset per root (rank space), for donated tasks
-  int static_chunk;            // warp w's first chunk: entries [w * static_chunk, +static_chunk)
-  int n_static;                // entries dealt statically (the cursor starts here)
+  int static_chunk;            // entries per warp dealt statically (at most CHUNK_MAX)
+  int n_static;                // entries [0, n_static) are dealt statically, warp w taking
+                               // w, w + T, w + 2T, ... (T warps): the heaviest entries of a
+                               // descending order land on different warps; the cursor starts
+                               // at n_static
 };
 
 // Select the j-th set bit of a register bitset.
@@ -459,6 +465,18 @@ __global__ void __launch_bounds__(256) clique_cached_kernel(const __grid_constan
   unsigned phase = 0;
   const int gw = blockIdx.x * (blockDim.x >> 5) + warp_in_block();
   const int total_warps = gridDim.x * (blockDim.x >> 5);
+  // per-block sums, flushed by one thread at exit (few global atomics per launch):
+  // [0] cliques, [1] tasks, [2] idle polls, [3] waiting ns; and the block's static entries
+  // finished, subtracted from `pending` by the last of its warps to finish its static chunk
+  __shared__ unsigned long long blk_sum[4];
+  __shared__ int blk_static_done, blk_warps_done;
+  if (threadIdx.x < 4) blk_sum[threadIdx.x] = 0ull;
+  if (threadIdx.x == 0) {
+    blk_static_done = 0;
+    blk_warps_done = 0;
+  }
+  __syncthreads();
+  unsigned long long idle[2] = {0ull, 0ull};
   int32_t* my_arena =
       a.c.arena ? a.c.arena + (size_t)gw * (32 / a.c.list_vwarp) * K * a.c.arena_dcap : nullptr;
   unsigned long long cnt = 0, ntasks = 0;
@@ -470,13 +488,15 @@ __global__ void __launch_bounds__(256) clique_cached_kernel(const __grid_constan
 #pragma unroll
     for (int j = 0; j < QPATH; ++j) path[j] = 0;
     bool donated = false;
+    const bool is_static = first_claim;
     if (lane == 0) {
-      if (first_claim && gw * a.static_chunk < a.n_static) {
-        first = gw * a.static_chunk;
-        count = min(a.static_chunk, a.n_static - first);
+      if (is_static) {
+        first = gw;
+        count = gw < a.n_static ? (a.n_static - gw + total_warps - 1) / total_warps : 0;
         ok = 1;
       } else {
-        ok = lb_next(a.c.lb, a.c.n_roots, total_warps, first, count, b, e, donated, level, path, &unflushed) ? 1 : 0;
+        ok = lb_next(a.c.lb, a.c.n_roots, total_warps, first, count, b, e, donated, level, path, &unflushed, idle)
+                 ? 1 : 0;
       }
     }
     first_claim = false;
@@ -505,7 +525,7 @@ __global__ void __launch_bounds__(256) clique_cached_kernel(const __grid_constan
         d = __ldg(a.c.g.deg + root);
         off = d >= 2 && d <= 64 * INDEX_MAX_WORDS ? __ldg(a.boff + root) : INDEX_NONE;
       } else {
-        const RootDesc rd = a.desc[first + lane];
+        const RootDesc rd = a.desc[is_static ? first + lane * total_warps : first + lane];
         root = rd.root;
         d = rd.d;
         off = rd.off;
@@ -567,13 +587,36 @@ __global__ void __launch_bounds__(256) clique_cached_kernel(const __grid_constan
       i0 = i1;
     }
     if (lane == 0) {
-      if (donated) lb_done(a.c.lb, 1);
-      else unflushed += count;
+      if (donated) {
+        lb_done(a.c.lb, 1);
+      } else if (is_static) {
+        // the block's last warp to finish its static chunk settles the whole block's
+        atomicAdd(&blk_static_done, count);
+        if (atomicAdd(&blk_warps_done, 1) == (int)(blockDim.x >> 5) - 1) {
+          __threadfence_block();
+          const int done = atomicAdd(&blk_static_done, 0);
+          if (done) lb_done(a.c.lb, done);
+        }
+      } else {
+        unflushed += count;
+      }
     }
   }
   if (lane == 0 && unflushed) lb_done(a.c.lb, unflushed);
-  dm_gpm::aggregate_counter<32>(&a.c.lb.ctr->count, cnt);
-  if (lane == 0) atomicAdd(&a.c.lb.ctr->tasks, ntasks);
+  cnt = warp_sum_u64(cnt);
+  if (lane == 0) {
+    atomicAdd(&blk_sum[0], cnt);
+    atomicAdd(&blk_sum[1], ntasks);
+    atomicAdd(&blk_sum[2], idle[0]);
+    atomicAdd(&blk_sum[3], idle[1]);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    if (blk_sum[0]) atomicAdd(&a.c.lb.ctr->count, blk_sum[0]);
+    atomicAdd(&a.c.lb.ctr->tasks, blk_sum[1]);
+    if (blk_sum[2]) atomicAdd(&a.c.lb.ctr->idle_polls, blk_sum[2]);
+    if (blk_sum[3]) atomicAdd(&a.c.lb.ctr->hungry_ns, blk_sum[3]);
+  }
 }
 
 }  // namespace dmb

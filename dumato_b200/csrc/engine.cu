@@ -9,12 +9,15 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
+#include <chrono>
 #include <climits>
 #include <cstring>
 #include <map>
 #include <mutex>
 #include <numeric>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "engine.hpp"
@@ -205,6 +208,82 @@ struct L2Window {
     cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, prev_limit);
     cudaGetLastError();
   }
+};
+
+// Live reports (dm_opts.report): while a counting kernel runs, a library thread copies the
+// call's counter block every report_ms on a stream of its own (non-blocking, so the copy
+// runs beside the kernel) into pinned memory and hands a dm_report to the caller's
+// function. The thread stops after the call's stream has been synchronised.
+static std::map<int, cudaStream_t> g_report_streams;
+
+class Reporter {
+ public:
+  int start(const dm_opts* o, int dev, const DevCounters* ctr, int warps, int64_t roots) {
+    if (!o || !o->report || o->report_ms <= 0) return DM_OK;
+    {
+      std::lock_guard<std::mutex> lk(g_dev_mu);
+      if (!g_report_streams.count(dev)) {
+        cudaStream_t s;
+        DM_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+        g_report_streams[dev] = s;
+      }
+      st_ = g_report_streams[dev];
+    }
+    DM_CUDA(cudaMallocHost(&snap_, sizeof(DevCounters)));
+    fn_ = o->report;
+    user_ = o->report_user;
+    ms_ = o->report_ms;
+    dev_ = dev;
+    ctr_ = ctr;
+    warps_ = warps;
+    roots_ = roots;
+    t0_ = std::chrono::steady_clock::now();
+    th_ = std::thread([this] { run(); });
+    return DM_OK;
+  }
+  ~Reporter() { stop(); }
+  void stop() {
+    if (th_.joinable()) {
+      done_ = true;
+      th_.join();
+    }
+    if (snap_) cudaFreeHost(snap_);
+    snap_ = nullptr;
+  }
+
+ private:
+  void run() {
+    cudaSetDevice(dev_);
+    while (!done_) {
+      std::this_thread::sleep_for(std::chrono::milliseconds(ms_));
+      if (done_) break;
+      if (cudaMemcpyAsync(snap_, ctr_, sizeof(DevCounters), cudaMemcpyDeviceToHost, st_) != cudaSuccess ||
+          cudaStreamSynchronize(st_) != cudaSuccess) {
+        cudaGetLastError();
+        break;
+      }
+      dm_report r{};
+      r.elapsed_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0_).count();
+      r.warps = warps_;
+      r.hungry_warps = std::max(0, std::min(warps_, snap_->hungry));
+      r.roots_claimed = std::min<int64_t>(roots_, snap_->cursor);
+      r.roots_total = roots_;
+      r.pending = snap_->pending;
+      r.donations = snap_->donations;
+      r.progress = snap_->progress;
+      fn_(&r, user_);
+    }
+  }
+  std::thread th_;
+  std::atomic<bool> done_{false};
+  DevCounters* snap_ = nullptr;
+  const DevCounters* ctr_ = nullptr;
+  cudaStream_t st_ = nullptr;
+  dm_report_fn fn_ = nullptr;
+  void* user_ = nullptr;
+  int ms_ = 0, dev_ = 0, warps_ = 0;
+  int64_t roots_ = 0;
+  std::chrono::steady_clock::time_point t0_;
 };
 
 // Workspaces of released graphs, per device, handed to the next graph that needs one on that
@@ -756,15 +835,19 @@ int dm_count_cliques(dm_graph* g, int32_t k, const dm_opts* o, uint64_t* count, 
   L.max_donations = ctx.donations_per_warp;
   int grid = 0, cursor = 0;
   if (use_index) {
+    // a root's block is staged in one round trip, so tasks are short: a task may donate
+    // after 2 us instead of 20
+    ctx.donate_after_us = std::min(ctx.donate_after_us, 2);
     L.desc = d_desc;
     L.blocks = s->d_blocks;
     L.boff = s->d_boff;
     L.tma = !(o && o->staging == DM_STAGE_LOADS);
     if (n_roots > 0) {
       if ((rc = clique_cached_grid(L, ctx, &grid))) return rc;
-      // every warp starts on a static chunk of the list: no cursor atomics at launch
+      // every warp starts on static entries of the list (w, w + T, ...): no cursor atomics
+      // while the first CHUNK_MAX x T entries are counted
       const int warps = grid * 8;
-      L.static_chunk = std::max(1, std::min(8, n_roots / std::max(warps, 1)));
+      L.static_chunk = std::max(1, std::min(16, (n_roots + warps - 1) / std::max(warps, 1)));
       L.n_static = (int)std::min<int64_t>(n_roots, (int64_t)warps * L.static_chunk);
       cursor = L.n_static;
     }
@@ -777,9 +860,11 @@ int dm_count_cliques(dm_graph* g, int32_t k, const dm_opts* o, uint64_t* count, 
     if (rc) return rc;
   }
   DM_CUDA(cudaEventRecord(ws.k0, ctx.stream));
+  Reporter reporter;
   if (n_roots > 0) {
     rc = use_index ? clique_cached_launch(L, ctx, grid) : clique_launch(L, ctx, &grid);
     if (rc) return rc;
+    if ((rc = reporter.start(o, ctx.device, ws.d_ctr, grid * 8, n_roots))) return rc;
   }
   DM_CUDA(cudaEventRecord(ws.k1, ctx.stream));
   DevCounters h;
@@ -978,9 +1063,11 @@ int dm_count_motifs(dm_graph* g, int32_t k, const dm_dictionary* dict, const dm_
     return rc;
   DM_CUDA(cudaEventRecord(ws.k0, ctx.stream));
   int grid = 0;
+  Reporter reporter;
   if (n_roots > 0) {
     rc = motif_launch(L, ctx, &grid);
     if (rc) return rc;
+    if ((rc = reporter.start(o, ctx.device, ws.d_ctr, grid * 8, n_roots))) return rc;
   }
   DM_CUDA(cudaEventRecord(ws.k1, ctx.stream));
   DevCounters h;

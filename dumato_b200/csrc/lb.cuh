@@ -173,9 +173,11 @@ static __device__ __noinline__ bool q_pop(const LBArgs& lb, int home, int& root,
 // error was raised. A caller that defers the pending-count decrements of the roots it has
 // finished passes their number in *unflushed: they are subtracted before the caller waits
 // for work (so `pending` can reach zero), and *unflushed is reset.
+// A caller that passes `idle` (polls, waiting ns) gets its waiting statistics added there
+// instead of to the global counters, to be summed per block at exit.
 static __device__ __noinline__ bool lb_next(const LBArgs& lb, int n_roots, int total_warps, int& first, int& count,
                                             int& b, int& e, bool& donated, int& level, int* path,
-                                            int* unflushed = nullptr) {
+                                            int* unflushed = nullptr, unsigned long long* idle = nullptr) {
   DevCounters* c = lb.ctr;
   int cur = vload(&c->cursor);
   if (cur < n_roots) {
@@ -203,7 +205,7 @@ static __device__ __noinline__ bool lb_next(const LBArgs& lb, int n_roots, int t
   long long t0 = t_hungry;
   unsigned long long last = vload64(&c->progress);
   int last_pending = vload(&c->pending);
-  unsigned backoff = 256;
+  unsigned backoff = 128;
   unsigned long long polls = 0;
   bool got = false;
   const int home = (int)((blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) % (unsigned)lb.nq);
@@ -241,11 +243,22 @@ static __device__ __noinline__ bool lb_next(const LBArgs& lb, int n_roots, int t
     }
     ++polls;
     __nanosleep(backoff);
-    if (backoff < 16384) backoff <<= 1;
+    // the back-off cap grows with the time spent waiting: short kernels see their end
+    // within about a microsecond, long waits poll the shared words at most every 16 us
+    const long long waited = global_ns() - t_hungry;
+    const unsigned cap = waited < 250000 ? 1024u : 16384u;
+    backoff = backoff < cap ? backoff << 1 : cap;
   }
-  atomicSub(&c->hungry, 1);
-  if (polls) atomicAdd(&c->idle_polls, polls);
-  atomicAdd(&c->hungry_ns, (unsigned long long)(global_ns() - t_hungry));
+  // a warp that leaves because all work is done need not withdraw its demand
+  if (got || !idle) atomicSub(&c->hungry, 1);
+  const unsigned long long waited_ns = (unsigned long long)(global_ns() - t_hungry);
+  if (idle) {
+    idle[0] += polls;
+    idle[1] += waited_ns;
+  } else {
+    if (polls) atomicAdd(&c->idle_polls, polls);
+    atomicAdd(&c->hungry_ns, waited_ns);
+  }
   return got;
 }
 

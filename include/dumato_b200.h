@@ -95,6 +95,20 @@ typedef struct dm_graph_info {
 #define DM_SCHED_LEARNED 1 /* roots ordered by the work predictor (needs a trained predictor) */
 #define DM_SCHED_ID 2      /* roots in id order (the reference's striping order) */
 
+/* A live sample of a running count (the reference's Report thread, src/main/Report.cpp:24-89,
+   which prints the share of active warps every interval). */
+typedef struct dm_report {
+  double elapsed_ms;           /* host time since the counting kernel was launched */
+  int32_t warps;               /* warps of the launch */
+  int32_t hungry_warps;        /* warps waiting for work when sampled */
+  int64_t roots_claimed;       /* root tasks dealt to warps so far */
+  int64_t roots_total;
+  int64_t pending;             /* root and donated tasks not settled */
+  uint64_t donations;          /* tasks donated between warps so far */
+  uint64_t progress;           /* work finished (advances while long items run) */
+} dm_report;
+typedef void (*dm_report_fn)(const dm_report* sample, void* user);
+
 typedef struct dm_opts {
   int32_t struct_size;
   int32_t device;              /* CUDA ordinal; -1 = current device */
@@ -119,7 +133,10 @@ typedef struct dm_opts {
   int32_t test_flags;          /* DM_TEST_* (tests of the failure paths only), else 0 */
   int32_t staging;             /* DM_STAGE_* (cliques on the index) */
   int32_t flags;               /* DM_FLAG_* */
-  int32_t reserved;
+  int32_t report_ms;           /* > 0 with report set: sampling interval of live reports */
+  dm_report_fn report;         /* called on a library thread every report_ms while a counting
+                                  kernel runs (optional) */
+  void* report_user;           /* passed to report */
 } dm_opts;
 
 /* flags: for the duration of the call, mark the graph's device CSR (and the clique index) as

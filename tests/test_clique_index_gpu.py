@@ -116,3 +116,20 @@ def test_index_rebuilt_after_release(dm, orc, gpu):
     for _ in range(3):
         assert dm.count_cliques(g, 3)[0] == want
         g.release_device()
+
+
+def test_live_reports_during_a_count(dm, orc, gpu):
+    """A report function set in the options is called every report_ms while the counting
+    kernel runs, with the warps' occupancy and the tasks dealt so far; counts are unchanged."""
+    from dumato_b200 import workloads
+
+    g = workloads.make("rmat100k", 1)
+    want = orc.clique_dag_bytes(_og(orc, g), 7)[0]
+    samples = []
+    got, st = dm.count_cliques(g, 7, dm.Options(threshold=100, report=samples.append, report_ms=2))
+    assert got == want
+    assert len(samples) >= 2, (len(samples), st.kernel_ms)
+    assert all(0 <= s["hungry_warps"] <= s["warps"] and s["roots_claimed"] <= s["roots_total"] for s in samples)
+    claimed = [s["roots_claimed"] for s in samples]
+    assert claimed == sorted(claimed)
+    assert [s["elapsed_ms"] for s in samples] == sorted(s["elapsed_ms"] for s in samples)
