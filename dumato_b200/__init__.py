@@ -140,6 +140,7 @@ _SIGNATURES = {
     "dm_count_cliques_noalloc": (ctypes.c_int, [_P, _P, _P, ctypes.c_int32, _P, ctypes.c_int32, ctypes.c_int32,
                                                 ctypes.c_int32, ctypes.c_uint64, _P]),
     "dm_count_cliques": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.POINTER(_Opts), _P, ctypes.POINTER(_Stats)]),
+    "dm_count_cliques_upto": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.POINTER(_Opts), _P, ctypes.POINTER(_Stats)]),
     "dm_count_motifs": (ctypes.c_int, [_P, ctypes.c_int32, _P, ctypes.POINTER(_Opts), _P, ctypes.POINTER(_Stats)]),
     "dm_batch_create": (ctypes.c_int, [ctypes.POINTER(_Query), ctypes.c_int32, ctypes.POINTER(_Opts), ctypes.c_int32,
                                        ctypes.POINTER(_P)]),
@@ -546,6 +547,15 @@ def count_cliques(g: Graph, k: int, opts: Optional[Options] = None) -> tuple[int
     st = _Stats()
     _check(lib().dm_count_cliques(g.handle, int(k), ctypes.byref(o), ctypes.byref(out), ctypes.byref(st)))
     return out.value, Stats.from_c(st)
+
+
+def count_cliques_upto(g: Graph, kmax: int, opts: Optional[Options] = None) -> tuple[dict, Stats]:
+    """Clique counts of every size 3..kmax from one traversal: ({k: count}, stats)."""
+    o = (opts or Options()).to_c()
+    out = np.zeros(kmax - 2, np.uint64)
+    st = _Stats()
+    _check(lib().dm_count_cliques_upto(g.handle, int(kmax), ctypes.byref(o), _ptr(out), ctypes.byref(st)))
+    return {k: int(out[k - 3]) for k in range(3, kmax + 1)}, Stats.from_c(st)
 
 
 def count_motifs(g: Graph, k: int, dictionary: Optional[Dictionary] = None,

@@ -26,15 +26,16 @@ static CliqueArgs clique_args(const CliqueLaunch& L, LaunchCtx& ctx) {
   return a;
 }
 
-static int cached_dispatch(CachedArgs* a, int k, int m, bool tma, LaunchCtx& ctx, int* grid, bool query) {
+static int cached_dispatch(CachedArgs* a, int k, int m, bool tma, bool multi, LaunchCtx& ctx, int* grid,
+                           bool query) {
   switch (k) {
-    case 2: return cached_nw<2>(a, m, tma, ctx, grid, query);
-    case 3: return cached_nw<3>(a, m, tma, ctx, grid, query);
-    case 4: return cached_nw<4>(a, m, tma, ctx, grid, query);
-    case 5: return cached_nw<5>(a, m, tma, ctx, grid, query);
-    case 6: return cached_nw<6>(a, m, tma, ctx, grid, query);
+    case 2: return cached_nw<2>(a, m, tma, multi, ctx, grid, query);
+    case 3: return cached_nw<3>(a, m, tma, multi, ctx, grid, query);
+    case 4: return cached_nw<4>(a, m, tma, multi, ctx, grid, query);
+    case 5: return cached_nw<5>(a, m, tma, multi, ctx, grid, query);
+    case 6: return cached_nw<6>(a, m, tma, multi, ctx, grid, query);
     case 7:
-    case 8: return clique_cached_k7_8(a, k, m, tma, ctx, grid, query);
+    case 8: return clique_cached_k7_8(a, k, m, tma, multi, ctx, grid, query);
     default: return fail(DM_EINVAL, "the clique index kernel covers k in [2, 8]");
   }
 }
@@ -53,13 +54,13 @@ static CachedArgs cached_args(const CliqueLaunch& L, LaunchCtx& ctx) {
 int clique_cached_grid(const CliqueLaunch& L, LaunchCtx& ctx, int* grid) {
   CachedArgs a = cached_args(L, ctx);
   *grid = 0;
-  return cached_dispatch(&a, L.k, L.nwmax, L.tma, ctx, grid, true);
+  return cached_dispatch(&a, L.k, L.nwmax, L.tma, L.multi, ctx, grid, true);
 }
 
 int clique_cached_launch(const CliqueLaunch& L, LaunchCtx& ctx, int grid) {
   CachedArgs a = cached_args(L, ctx);
   int g = grid;
-  return cached_dispatch(&a, L.k, L.nwmax, L.tma, ctx, &g, false);
+  return cached_dispatch(&a, L.k, L.nwmax, L.tma, L.multi, ctx, &g, false);
 }
 
 template <int M>

@@ -250,13 +250,105 @@ struct TaskWords {
   int* heavy;                 // their item indices
 };
 
+// Per-lane clique counts by size (the fused count of every k up to K): c[s] = s-cliques.
+template <int K>
+struct Acc {
+  unsigned long long c[K + 1];
+};
+
+// Fused counting below a candidate set S whose members would be the S0-th vertex of a clique:
+// c[S0] += |S|, and for every x in S the cliques of S_{>x} & N(x) count at S0 + 1, down to
+// c[S0 + L]. Unlike count_rec no subtree is pruned for being too small to reach K, since its
+// smaller cliques count too.
+template <int L, int NW, int K, int S0>
+__device__ __forceinline__ void count_all(const Bits<NW>& S, const uint64_t* __restrict__ rows, Acc<K>& acc) {
+  acc.c[S0] += (unsigned long long)popc(S);
+  if constexpr (L > 0) {
+#pragma unroll
+    for (int wi = 0; wi < NW; ++wi) {
+      uint64_t bits = S.w[wi];
+      while (bits) {
+        const int b = __ffsll((long long)bits) - 1;
+        bits &= bits - 1;
+        const uint64_t* rc = rows + (wi * 64 + b) * NW;
+        Bits<NW> T;
+        uint64_t any = 0;
+#pragma unroll
+        for (int j = 0; j < NW; ++j) {
+          T.w[j] = (j < wi ? 0ull : (j == wi ? bits : S.w[j])) & rc[j];
+          any |= T.w[j];
+        }
+        if (any) count_all<L - 1, NW, K, S0 + 1>(T, rows, acc);
+      }
+    }
+  }
+}
+
+// count_all at the top of a long item, moving the load balancer's watched word every 16
+// subtrees (see count_rec_hb).
+template <int L, int NW, int K, int S0>
+__device__ __forceinline__ void count_all_hb(const Bits<NW>& S, const uint64_t* __restrict__ rows, Acc<K>& acc,
+                                             unsigned long long* progress) {
+  if constexpr (L < 3) {
+    count_all<L, NW, K, S0>(S, rows, acc);
+  } else {
+    acc.c[S0] += (unsigned long long)popc(S);
+    unsigned sub = 0;
+#pragma unroll
+    for (int wi = 0; wi < NW; ++wi) {
+      uint64_t bits = S.w[wi];
+      while (bits) {
+        const int b = __ffsll((long long)bits) - 1;
+        bits &= bits - 1;
+        const uint64_t* rc = rows + (wi * 64 + b) * NW;
+        Bits<NW> T;
+        uint64_t any = 0;
+#pragma unroll
+        for (int j = 0; j < NW; ++j) {
+          T.w[j] = (j < wi ? 0ull : (j == wi ? bits : S.w[j])) & rc[j];
+          any |= T.w[j];
+        }
+        if (any) count_all<L - 1, NW, K, S0 + 1>(T, rows, acc);
+        if ((++sub & 15) == 0) atomicAdd(progress, 1ull);
+      }
+    }
+  }
+}
+
+// Fused counting of item `it` (the local edge c1 < c2 of the root): the item is a triangle,
+// its candidate set S = row[c1] & row[c2] holds the 4-cliques, and so on down to K. For
+// K >= 6 an item with a large S is deferred to the warp after its 4-cliques are counted.
+template <int K, int NW>
+__device__ __forceinline__ void bitmap_item_all(int it, const uint64_t* rows, const int32_t* sE, int d, int* hn,
+                                                int* heavy, unsigned long long* progress, Acc<K>& acc) {
+  acc.c[3] += 1ull;
+  const int c1 = lower_bound(sE, 0, d + 1, it + 1) - 1;
+  const int c2 = select_bit<NW>(rows + c1 * NW, it - sE[c1]);
+  Bits<NW> S;
+#pragma unroll
+  for (int w = 0; w < NW; ++w) S.w[w] = rows[c1 * NW + w] & rows[c2 * NW + w];
+  if constexpr (K >= 6) {
+    const int p = popc(S);
+    if (p >= HEAVY_BITS && hn) {
+      const int slot = atomicAdd(hn, 1);
+      if (slot < HEAVY_SLOTS) {
+        heavy[slot] = it;
+        acc.c[4] += (unsigned long long)p;
+        return;
+      }
+    }
+  }
+  count_all_hb<K - 4, NW, K, 4>(S, rows, acc, progress);
+}
+
 // Level-1 task: positions [lo, hi) (hi < 0: to the end) of the candidate set S of item
 // `it` choose the third local vertex c3; each lane counts the (k-3)-cliques of
 // S_{>c3} & row[c3] for the positions it takes. While warps are hungry the upper half of
 // the positions left is donated as (root, level 1, path = {it}, range).
-template <int K, int NW>
+template <int K, int NW, bool MULTI>
 __device__ unsigned long long heavy_run(const CachedArgs& a, const TaskWords& tw, const uint64_t* rows,
-                                        const int32_t* sE, int d, int root, int it, int lo, int hi, bool eager) {
+                                        const int32_t* sE, int d, int root, int it, int lo, int hi, bool eager,
+                                        Acc<K>& acc) {
   const int lane = lane_id();
   const int c1 = lower_bound(sE, 0, d + 1, it + 1) - 1;
   const int c2 = select_bit<NW>(rows + c1 * NW, it - sE[c1]);
@@ -284,7 +376,8 @@ __device__ unsigned long long heavy_run(const CachedArgs& a, const TaskWords& tw
     Bits<NW> T;
 #pragma unroll
     for (int w = 0; w < NW; ++w) T.w[w] = (w < w3 ? 0ull : (w == w3 ? (S.w[w] & above) : S.w[w])) & rc[w];
-    if (popc(T) >= K - 4) cnt += count_rec_hb<(K >= 6 ? K - 5 : 0), NW>(T, rows, &a.c.lb.ctr->progress);
+    if constexpr (MULTI) count_all_hb<K - 5, NW, K, 5>(T, rows, acc, &a.c.lb.ctr->progress);
+    else if (popc(T) >= K - 4) cnt += count_rec_hb<(K >= 6 ? K - 5 : 0), NW>(T, rows, &a.c.lb.ctr->progress);
     // every position is a whole subtree below level 2: check for hungry warps after each
     {
       int ob = 0, oe = 0;
@@ -296,7 +389,8 @@ __device__ unsigned long long heavy_run(const CachedArgs& a, const TaskWords& tw
           Bits<NW> U;
 #pragma unroll
           for (int w = 0; w < NW; ++w) U.w[w] = (w < wq ? 0ull : (w == wq ? (S.w[w] & ab) : S.w[w])) & rows[c * NW + w];
-          if (popc(U) >= K - 4) cnt += count_rec_hb<(K >= 6 ? K - 5 : 0), NW>(U, rows, &a.c.lb.ctr->progress);
+          if constexpr (MULTI) count_all_hb<K - 5, NW, K, 5>(U, rows, acc, &a.c.lb.ctr->progress);
+          else if (popc(U) >= K - 4) cnt += count_rec_hb<(K >= 6 ? K - 5 : 0), NW>(U, rows, &a.c.lb.ctr->progress);
         }
       }
     }
@@ -308,9 +402,10 @@ __device__ unsigned long long heavy_run(const CachedArgs& a, const TaskWords& tw
 // Counts one root's task from its staged rows: level 0 runs items [b, e) (task_range
 // encoding; items are the local edges, or the rows when k == 3), level 1 runs positions
 // [b, e) of item `it`'s candidate set. Returns this lane's share.
-template <int K, int NW>
+template <int K, int NW, bool MULTI>
 __device__ unsigned long long staged_run(const CachedArgs& a, const TaskWords& tw, const uint64_t* rows,
-                                         int32_t* sE, int root, int d, int b, int e, int level, int it, bool eager) {
+                                         int32_t* sE, int root, int d, int b, int e, int level, int it, bool eager,
+                                         Acc<K>& acc) {
   const int lane = lane_id();
   int n_items;
   if constexpr (K >= 4) {
@@ -338,7 +433,7 @@ __device__ unsigned long long staged_run(const CachedArgs& a, const TaskWords& t
   }
   __syncwarp();
   if constexpr (K >= 6) {
-    if (level == 1) return heavy_run<K, NW>(a, tw, rows, sE, d, root, it, b, e, eager);
+    if (level == 1) return heavy_run<K, NW, MULTI>(a, tw, rows, sE, d, root, it, b, e, eager, acc);
   }
   int lo, hi;
   task_range(b, e, n_items, lo, hi);
@@ -354,11 +449,15 @@ __device__ unsigned long long staged_run(const CachedArgs& a, const TaskWords& t
   unsigned done = 0;
   int x;
   while ((x = range_take(tw.range)) >= 0) {
-    cnt += bitmap_item<K, NW>(x, rows, sE, d, tw.hn, tw.heavy, &a.c.lb.ctr->progress);
+    if constexpr (MULTI) bitmap_item_all<K, NW>(x, rows, sE, d, tw.hn, tw.heavy, &a.c.lb.ctr->progress, acc);
+    else cnt += bitmap_item<K, NW>(x, rows, sE, d, tw.hn, tw.heavy, &a.c.lb.ctr->progress);
     if ((++done & 15) == 0) {
       int ob = 0, oe = 0;
       if (range_maybe_donate(a.c.lb, tw.range, root, tw.don, t_start, tw.busy, ob, oe, 0, 0, 0, nullptr, eager)) {
-        for (int j = ob; j < oe; ++j) cnt += bitmap_item<K, NW>(j, rows, sE, d, nullptr, nullptr, &a.c.lb.ctr->progress);
+        for (int j = ob; j < oe; ++j) {
+          if constexpr (MULTI) bitmap_item_all<K, NW>(j, rows, sE, d, nullptr, nullptr, &a.c.lb.ctr->progress, acc);
+          else cnt += bitmap_item<K, NW>(j, rows, sE, d, nullptr, nullptr, &a.c.lb.ctr->progress);
+        }
       }
       if ((done & 255) == 0) atomicAdd(&a.c.lb.ctr->progress, 256ull);
     }
@@ -368,24 +467,25 @@ __device__ unsigned long long staged_run(const CachedArgs& a, const TaskWords& t
     const int nh = min(*tw.hn, HEAVY_SLOTS);
     for (int h = 0; h < nh; ++h) {
       const int hit = tw.heavy[h];
-      cnt += heavy_run<K, NW>(a, tw, rows, sE, d, root, hit, 0, -1, eager);
+      cnt += heavy_run<K, NW, MULTI>(a, tw, rows, sE, d, root, hit, 0, -1, eager, acc);
     }
   }
   return cnt;
 }
 
-template <int K, int M>
+template <int K, int M, bool MULTI>
 __device__ __forceinline__ unsigned long long staged_dispatch(const CachedArgs& a, const TaskWords& tw,
                                                               const uint64_t* rows, int32_t* sE, int root, int d,
-                                                              int b, int e, int level, int it, bool eager) {
+                                                              int b, int e, int level, int it, bool eager,
+                                                              Acc<K>& acc) {
   const int nw = (d + 63) >> 6;
-  if (nw <= 1) return staged_run<K, 1>(a, tw, rows, sE, root, d, b, e, level, it, eager);
+  if (nw <= 1) return staged_run<K, 1, MULTI>(a, tw, rows, sE, root, d, b, e, level, it, eager, acc);
   if constexpr (M >= 2)
-    if (nw == 2) return staged_run<K, 2>(a, tw, rows, sE, root, d, b, e, level, it, eager);
+    if (nw == 2) return staged_run<K, 2, MULTI>(a, tw, rows, sE, root, d, b, e, level, it, eager, acc);
   if constexpr (M >= 3)
-    if (nw == 3) return staged_run<K, 3>(a, tw, rows, sE, root, d, b, e, level, it, eager);
+    if (nw == 3) return staged_run<K, 3, MULTI>(a, tw, rows, sE, root, d, b, e, level, it, eager, acc);
   if constexpr (M >= 4)
-    if (nw == 4) return staged_run<K, 4>(a, tw, rows, sE, root, d, b, e, level, it, eager);
+    if (nw == 4) return staged_run<K, 4, MULTI>(a, tw, rows, sE, root, d, b, e, level, it, eager, acc);
   if (lane_id() == 0) set_err(a.c.lb.ctr, ERR_BAD_TASK);
   return 0;
 }
@@ -444,7 +544,7 @@ __device__ __forceinline__ bool stage_blocks(const uint4* blocks, uint4* stage, 
   }
 }
 
-template <int K, int M, bool TMA>
+template <int K, int M, bool TMA, bool MULTI>
 __global__ void __launch_bounds__(256) clique_cached_kernel(const __grid_constant__ CachedArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
   constexpr CachedWarp LY = cached_layout(M);
@@ -469,14 +569,19 @@ __global__ void __launch_bounds__(256) clique_cached_kernel(const __grid_constan
   // [0] cliques, [1] tasks, [2] idle polls, [3] waiting ns; and the block's static entries
   // finished, subtracted from `pending` by the last of its warps to finish its static chunk
   __shared__ unsigned long long blk_sum[4];
+  __shared__ unsigned long long blk_k[16];  // fused counts by clique size
   __shared__ int blk_static_done, blk_warps_done;
   if (threadIdx.x < 4) blk_sum[threadIdx.x] = 0ull;
+  if (MULTI && threadIdx.x < 16) blk_k[threadIdx.x] = 0ull;
   if (threadIdx.x == 0) {
     blk_static_done = 0;
     blk_warps_done = 0;
   }
   __syncthreads();
   unsigned long long idle[2] = {0ull, 0ull};
+  Acc<K> acc;
+#pragma unroll
+  for (int j = 0; j <= K; ++j) acc.c[j] = 0ull;
   int32_t* my_arena =
       a.c.arena ? a.c.arena + (size_t)gw * (32 / a.c.list_vwarp) * K * a.c.arena_dcap : nullptr;
   unsigned long long cnt = 0, ntasks = 0;
@@ -569,7 +674,9 @@ __global__ void __launch_bounds__(256) clique_cached_kernel(const __grid_constan
         } else if (K == 2) {
           if (lane == 0) tc = (unsigned long long)di;
         } else if (ui > 0) {
-          tc = staged_dispatch<K, M>(a, tw, srows + 2 * si, sE, r, di, bb, ee, level, it1, eager);
+          tc = staged_dispatch<K, M, MULTI>(a, tw, srows + 2 * si, sE, r, di, bb, ee, level, it1, eager, acc);
+        } else if (MULTI && di > a.c.list_threshold) {
+          if (lane == 0) set_err(a.c.lb.ctr, ERR_BAD_TASK);  // the fused count runs on the index only
         } else if (di > a.c.list_threshold) {
           if (K > 3 && (!my_arena || di > a.c.arena_dcap)) {
             if (lane == 0) set_err(a.c.lb.ctr, ERR_ARENA_OVERFLOW);
@@ -603,6 +710,14 @@ __global__ void __launch_bounds__(256) clique_cached_kernel(const __grid_constan
     }
   }
   if (lane == 0 && unflushed) lb_done(a.c.lb, unflushed);
+  if constexpr (MULTI) {
+#pragma unroll
+    for (int j = 3; j <= K; ++j) {
+      const unsigned long long v = warp_sum_u64(acc.c[j]);
+      if (lane == 0 && v) atomicAdd(&blk_k[j], v);
+    }
+    cnt = acc.c[K];
+  }
   cnt = warp_sum_u64(cnt);
   if (lane == 0) {
     atomicAdd(&blk_sum[0], cnt);
@@ -616,6 +731,10 @@ __global__ void __launch_bounds__(256) clique_cached_kernel(const __grid_constan
     atomicAdd(&a.c.lb.ctr->tasks, blk_sum[1]);
     if (blk_sum[2]) atomicAdd(&a.c.lb.ctr->idle_polls, blk_sum[2]);
     if (blk_sum[3]) atomicAdd(&a.c.lb.ctr->hungry_ns, blk_sum[3]);
+    if constexpr (MULTI) {
+      for (int j = 3; j <= K; ++j)
+        if (blk_k[j]) atomicAdd(&a.c.lb.ctr->count_k[j], blk_k[j]);
+    }
   }
 }
 

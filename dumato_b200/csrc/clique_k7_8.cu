@@ -8,8 +8,8 @@ int clique_launch_k7_8(const CliqueArgs& a, int k, int m, LaunchCtx& ctx, int* g
   return k == 7 ? launch_nw<7>(a, m, ctx, grid) : launch_nw<8>(a, m, ctx, grid);
 }
 
-int clique_cached_k7_8(CachedArgs* a, int k, int m, bool tma, LaunchCtx& ctx, int* grid, bool query) {
-  return k == 7 ? cached_nw<7>(a, m, tma, ctx, grid, query) : cached_nw<8>(a, m, tma, ctx, grid, query);
+int clique_cached_k7_8(CachedArgs* a, int k, int m, bool tma, bool multi, LaunchCtx& ctx, int* grid, bool query) {
+  return k == 7 ? cached_nw<7>(a, m, tma, multi, ctx, grid, query) : cached_nw<8>(a, m, tma, multi, ctx, grid, query);
 }
 
 }  // namespace dmb

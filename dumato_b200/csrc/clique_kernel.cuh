@@ -62,9 +62,9 @@ template <int K, int M>
 static int launch_k(const CliqueArgs& a, LaunchCtx& ctx, int* grid_out) {
   const size_t smem = (size_t)warp_layout(M).total * (CLIQUE_BLOCK / 32);
   auto kern = clique_kernel<K, M>;
-  DM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  static LaunchCache cache;
   int occ = 0;
-  DM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, CLIQUE_BLOCK, smem));
+  DM_CUDA(cached_occupancy(cache, kern, ctx.device, CLIQUE_BLOCK, smem, &occ));
   if (occ < 1) return fail(DM_EINVAL, "clique kernel does not fit on an SM");
   int grid = ctx.num_sms * occ;
   if (ctx.threads > 0) grid = std::max(1, std::min(grid, (ctx.threads + CLIQUE_BLOCK - 1) / CLIQUE_BLOCK));
@@ -91,13 +91,13 @@ static int launch_nw(const CliqueArgs& a, int m, LaunchCtx& ctx, int* grid) {
 }
 
 // Index-counting kernel: with query set, only the grid is computed.
-template <int K, int M, bool TMA>
+template <int K, int M, bool TMA, bool MULTI>
 static int cached_k(CachedArgs* a, LaunchCtx& ctx, int* grid_out, bool query) {
   const size_t smem = (size_t)cached_layout(M).total * (CLIQUE_BLOCK / 32);
-  auto kern = clique_cached_kernel<K, M, TMA>;
-  DM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  auto kern = clique_cached_kernel<K, M, TMA, MULTI>;
+  static LaunchCache cache;
   int occ = 0;
-  DM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, CLIQUE_BLOCK, smem));
+  DM_CUDA(cached_occupancy(cache, kern, ctx.device, CLIQUE_BLOCK, smem, &occ));
   if (occ < 1) return fail(DM_EINVAL, "clique index kernel does not fit on an SM");
   int grid = ctx.num_sms * occ;
   if (ctx.threads > 0) grid = std::max(1, std::min(grid, (ctx.threads + CLIQUE_BLOCK - 1) / CLIQUE_BLOCK));
@@ -114,18 +114,28 @@ static int cached_k(CachedArgs* a, LaunchCtx& ctx, int* grid_out, bool query) {
   return DM_OK;
 }
 
+// Fused counts (every size up to K) are staged by bulk copies only.
+template <int K, int M>
+static int cached_m(CachedArgs* a, bool tma, bool multi, LaunchCtx& ctx, int* grid, bool query) {
+  if (multi) {
+    if constexpr (K >= 4) return cached_k<K, M, true, true>(a, ctx, grid, query);
+    else return fail(DM_EINVAL, "fused clique counts need k >= 4");
+  }
+  return tma ? cached_k<K, M, true, false>(a, ctx, grid, query) : cached_k<K, M, false, false>(a, ctx, grid, query);
+}
+
 template <int K>
-static int cached_nw(CachedArgs* a, int m, bool tma, LaunchCtx& ctx, int* grid, bool query) {
+static int cached_nw(CachedArgs* a, int m, bool tma, bool multi, LaunchCtx& ctx, int* grid, bool query) {
   switch (m) {
-    case 1: return tma ? cached_k<K, 1, true>(a, ctx, grid, query) : cached_k<K, 1, false>(a, ctx, grid, query);
-    case 2: return tma ? cached_k<K, 2, true>(a, ctx, grid, query) : cached_k<K, 2, false>(a, ctx, grid, query);
-    case 3: return tma ? cached_k<K, 3, true>(a, ctx, grid, query) : cached_k<K, 3, false>(a, ctx, grid, query);
-    default: return tma ? cached_k<K, 4, true>(a, ctx, grid, query) : cached_k<K, 4, false>(a, ctx, grid, query);
+    case 1: return cached_m<K, 1>(a, tma, multi, ctx, grid, query);
+    case 2: return cached_m<K, 2>(a, tma, multi, ctx, grid, query);
+    case 3: return cached_m<K, 3>(a, tma, multi, ctx, grid, query);
+    default: return cached_m<K, 4>(a, tma, multi, ctx, grid, query);
   }
 }
 
 // Launchers of the k ranges compiled in the other translation units.
-int clique_cached_k7_8(CachedArgs* a, int k, int m, bool tma, LaunchCtx& ctx, int* grid, bool query);
+int clique_cached_k7_8(CachedArgs* a, int k, int m, bool tma, bool multi, LaunchCtx& ctx, int* grid, bool query);
 
 int clique_launch_k7_8(const CliqueArgs& a, int k, int m, LaunchCtx& ctx, int* grid);
 int clique_launch_k9(const CliqueArgs& a, int m, LaunchCtx& ctx, int* grid);

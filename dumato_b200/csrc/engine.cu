@@ -61,6 +61,8 @@ struct Workspace {
   RootDesc* d_sdesc = nullptr;
   size_t sdesc_cap = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, k0 = nullptr, k1 = nullptr;
+  DevCounters* h_init = nullptr;    // pinned: a call's initial counters (asynchronous upload)
+  DevCounters* h_out = nullptr;     // pinned: the counters read back after the kernel
 };
 
 
@@ -313,6 +315,8 @@ static void free_workspace(Workspace& w) {
   if (w.ev1) cudaEventDestroy(w.ev1);
   if (w.k0) cudaEventDestroy(w.k0);
   if (w.k1) cudaEventDestroy(w.k1);
+  if (w.h_init) cudaFreeHost(w.h_init);
+  if (w.h_out) cudaFreeHost(w.h_out);
   w = Workspace();
 }
 
@@ -392,6 +396,8 @@ static int ensure_ws_bytes(void** p, size_t* cap, size_t want) {
 
 static int prepare_ws(Workspace& ws, cudaStream_t st) {
   if (!ws.d_ctr) DM_CUDA(cudaMalloc(&ws.d_ctr, sizeof(DevCounters)));
+  if (!ws.h_init) DM_CUDA(cudaMallocHost(&ws.h_init, sizeof(DevCounters)));
+  if (!ws.h_out) DM_CUDA(cudaMallocHost(&ws.h_out, sizeof(DevCounters)));
   if (!ws.ev0) {
     DM_CUDA(cudaEventCreate(&ws.ev0));
     DM_CUDA(cudaEventCreate(&ws.ev1));
@@ -410,12 +416,14 @@ static int prepare_ws(Workspace& ws, cudaStream_t st) {
 
 // Initial counters: every root task is pending until a warp finishes it; the root cursor
 // starts after the entries dealt statically.
+// (pinned source: the copy is asynchronous; the previous call's copies have completed, since
+// every call ends by synchronising its stream)
 static int init_counters(Workspace& ws, int n_roots, cudaStream_t st, int cursor = 0) {
-  DevCounters h;
-  std::memset(&h, 0, sizeof(h));
-  h.pending = n_roots;
-  h.cursor = cursor;
-  DM_CUDA(cudaMemcpyAsync(ws.d_ctr, &h, sizeof(h), cudaMemcpyHostToDevice, st));
+  DevCounters* h = ws.h_init;
+  std::memset(h, 0, sizeof(DevCounters));
+  h->pending = n_roots;
+  h->cursor = cursor;
+  DM_CUDA(cudaMemcpyAsync(ws.d_ctr, h, sizeof(DevCounters), cudaMemcpyHostToDevice, st));
   return DM_OK;
 }
 
@@ -700,7 +708,12 @@ int dm_graph_release_device(dm_graph* g) {
   return DM_OK;
 }
 
-int dm_count_cliques(dm_graph* g, int32_t k, const dm_opts* o, uint64_t* count, dm_stats* st) {
+// One clique count (upto == nullptr) or the fused count of every size 3..k into upto[0..k-3].
+// Returns 1, having counted nothing, when the fused walk cannot run on this graph and call
+// (no clique index, roots above 256 out-neighbours, a per-launch or list mode, or a subtree
+// log), so that the caller counts size by size instead.
+static int count_cliques_impl(dm_graph* g, int32_t k, const dm_opts* o, uint64_t* count, dm_stats* st,
+                              uint64_t* upto) {
   if (!g || !count) return fail(DM_EINVAL, "dm_count_cliques: null argument");
   if (k < 2 || k > 12) return fail(DM_EINVAL, "dm_count_cliques: k must be in [2, 12]");
   int rc = check_opts(o);
@@ -722,7 +735,7 @@ int dm_count_cliques(dm_graph* g, int32_t k, const dm_opts* o, uint64_t* count, 
     s->dg.has_oriented = true;
   }
   // tasks: roots (rank space) with at least k-1 out-neighbours
-  const int need = k - 1;
+  const int need = upto ? 2 : k - 1;  // a fused count starts from every root with a local edge
   const int sched = o ? o->scheduler : DM_SCHED_PLAIN;
   const int world = (o && o->world_size > 1) ? o->world_size : 1;
   if ((rc = ensure_deg_order(g, s, ctx.stream))) return rc;
@@ -787,6 +800,7 @@ int dm_count_cliques(dm_graph* g, int32_t k, const dm_opts* o, uint64_t* count, 
     }
   }
   const bool use_index = want_index && s->index_state == 1 && d_desc != nullptr;
+  if (upto && (!use_index || max_d > INDEX_MAX_DEGREE || (o && o->subtree_counts))) return 1;
   CliqueLaunch L;
   L.k = k;
   if (mode == DM_MODE_LIST) {
@@ -838,6 +852,7 @@ int dm_count_cliques(dm_graph* g, int32_t k, const dm_opts* o, uint64_t* count, 
     // a root's block is staged in one round trip, so tasks are short: a task may donate
     // after 2 us instead of 20
     ctx.donate_after_us = std::min(ctx.donate_after_us, 2);
+    L.multi = upto != nullptr;
     L.desc = d_desc;
     L.blocks = s->d_blocks;
     L.boff = s->d_boff;
@@ -867,8 +882,7 @@ int dm_count_cliques(dm_graph* g, int32_t k, const dm_opts* o, uint64_t* count, 
     if ((rc = reporter.start(o, ctx.device, ws.d_ctr, grid * 8, n_roots))) return rc;
   }
   DM_CUDA(cudaEventRecord(ws.k1, ctx.stream));
-  DevCounters h;
-  DM_CUDA(cudaMemcpyAsync(&h, ws.d_ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost, ctx.stream));
+  DM_CUDA(cudaMemcpyAsync(ws.h_out, ws.d_ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost, ctx.stream));
   std::vector<unsigned long long> per_rank;
   if (want_log) {
     per_rank.resize(g->n);
@@ -877,6 +891,7 @@ int dm_count_cliques(dm_graph* g, int32_t k, const dm_opts* o, uint64_t* count, 
                               ctx.stream));
   }
   DM_CUDA(cudaStreamSynchronize(ctx.stream));
+  const DevCounters h = *ws.h_out;
   if ((rc = reset_queue(ws, h, ctx.stream))) return rc;
   float kms = 0, pms = 0;
   cudaEventElapsedTime(&kms, ws.k0, ws.k1);
@@ -885,6 +900,10 @@ int dm_count_cliques(dm_graph* g, int32_t k, const dm_opts* o, uint64_t* count, 
     return fail(kernel_status(h.err),
                 "clique kernel reported error " + std::to_string(h.err));
   *count = h.count;
+  if (upto) {
+    for (int j = 3; j <= k; ++j) upto[j - 3] = h.count_k[j];
+    *count = h.count_k[k];
+  }
   if (want_log)
     for (int32_t v = 0; v < g->n; ++v) o->subtree_counts[v] = per_rank[g->rank[v]];
   if (st) {
@@ -906,6 +925,38 @@ int dm_count_cliques(dm_graph* g, int32_t k, const dm_opts* o, uint64_t* count, 
     st->max_task_root = h.max_task_root;
     st->prefix_donations = (int32_t)std::min<unsigned long long>(h.prefix_donations, INT32_MAX);
   }
+  return DM_OK;
+}
+
+int dm_count_cliques(dm_graph* g, int32_t k, const dm_opts* o, uint64_t* count, dm_stats* st) {
+  return count_cliques_impl(g, k, o, count, st, nullptr);
+}
+
+int dm_count_cliques_upto(dm_graph* g, int32_t kmax, const dm_opts* o, uint64_t* counts, dm_stats* st) {
+  if (!g || !counts) return fail(DM_EINVAL, "dm_count_cliques_upto: null argument");
+  if (kmax < 4 || kmax > INDEX_MAX_K) return fail(DM_EINVAL, "dm_count_cliques_upto: kmax must be in [4, 8]");
+  uint64_t top = 0;
+  int rc = count_cliques_impl(g, kmax, o, &top, st, counts);
+  if (rc != 1) return rc;
+  // one launch per size
+  dm_stats sum{}, one{};
+  for (int k = 3; k <= kmax; ++k) {
+    if ((rc = count_cliques_impl(g, k, o, &counts[k - 3], st ? &one : nullptr, nullptr))) return rc;
+    if (st) {
+      if (k == 3) sum = one;
+      else {
+        sum.kernel_ms += one.kernel_ms;
+        sum.prep_ms += one.prep_ms;
+        sum.tasks += one.tasks;
+        sum.donations += one.donations;
+        sum.idle_polls += one.idle_polls;
+        sum.kernel_launches += one.kernel_launches;
+        sum.prefix_donations += one.prefix_donations;
+        sum.max_task_ms = std::max(sum.max_task_ms, one.max_task_ms);
+      }
+    }
+  }
+  if (st) *st = sum;
   return DM_OK;
 }
 
@@ -1070,14 +1121,14 @@ int dm_count_motifs(dm_graph* g, int32_t k, const dm_dictionary* dict, const dm_
     if ((rc = reporter.start(o, ctx.device, ws.d_ctr, grid * 8, n_roots))) return rc;
   }
   DM_CUDA(cudaEventRecord(ws.k1, ctx.stream));
-  DevCounters h;
-  DM_CUDA(cudaMemcpyAsync(&h, ws.d_ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost, ctx.stream));
+  DM_CUDA(cudaMemcpyAsync(ws.h_out, ws.d_ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost, ctx.stream));
   DM_CUDA(cudaMemcpyAsync(class_counts, ws.d_hist, sizeof(unsigned long long) * dict->n_classes,
                           cudaMemcpyDeviceToHost, ctx.stream));
   if (want_log && g->n)
     DM_CUDA(cudaMemcpyAsync(o->subtree_counts, ws.d_per_root, sizeof(unsigned long long) * g->n,
                             cudaMemcpyDeviceToHost, ctx.stream));
   DM_CUDA(cudaStreamSynchronize(ctx.stream));
+  const DevCounters h = *ws.h_out;
   if (h.err && d_bits) {
     // a failed launch can leave bits set: clear them for the next call
     DM_CUDA(cudaMemsetAsync(ws.d_bits, 0, ws.bits_cap, ctx.stream));

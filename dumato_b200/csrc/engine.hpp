@@ -32,6 +32,7 @@ struct alignas(128) DevCounters {
   unsigned long long hungry_ns;  // time warps spent waiting for work, summed over warps
   unsigned long long max_task_ns;  // longest single task
   unsigned long long prefix_donations;  // donated DFS prefixes (a level >= 1 extension set)
+  unsigned long long count_k[16];  // fused counts: cliques of every size up to k
   int max_task_root;             // its root (best effort under races)
   int test_gate;                 // never written by the library (failure-path tests)
   int err;                       // first error code raised by a kernel (0 = none)
@@ -142,6 +143,7 @@ struct CliqueLaunch {
   int static_chunk = 1;             // warp w starts with entries [w * static_chunk, +static_chunk)
   int n_static = 0;                 // entries dealt statically; the root cursor starts here
   bool tma = true;                  // stage blocks by bulk asynchronous copies (else 16-byte loads)
+  bool multi = false;               // fused: count every clique size up to k (count_k)
 };
 int clique_launch(const CliqueLaunch& L, LaunchCtx& ctx, int* grid);
 int clique_max_warps(int num_sms);
@@ -181,6 +183,29 @@ int motif_launch(const MotifLaunch& L, LaunchCtx& ctx, int* grid);
 size_t motif_arena_stride(int k, int maxdeg, int vwarp);  // int2 slots per warp
 
 const char* cuda_err_str(cudaError_t e);
+
+// Launch configuration of one kernel, settled once per device: the dynamic shared-memory
+// attribute is set and the resident blocks per SM are queried on the first launch only, so
+// a call spends no driver time on them afterwards.
+constexpr int LAUNCH_CACHE_DEVICES = 64;
+struct LaunchCache {
+  int smem[LAUNCH_CACHE_DEVICES] = {};
+  int occ[LAUNCH_CACHE_DEVICES] = {};
+};
+template <typename Kern>
+inline cudaError_t cached_occupancy(LaunchCache& c, Kern kern, int device, int block, size_t smem, int* occ) {
+  if (device >= 0 && device < LAUNCH_CACHE_DEVICES && c.occ[device] > 0 && c.smem[device] == (int)smem) {
+    *occ = c.occ[device];
+    return cudaSuccess;
+  }
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, kern, block, smem);
+  if (e == cudaSuccess && device >= 0 && device < LAUNCH_CACHE_DEVICES) {
+    c.smem[device] = (int)smem;
+    c.occ[device] = *occ;
+  }
+  return e;
+}
 
 // Host helpers shared by the entry points (engine.cu).
 int select_device(const dm_opts* o, LaunchCtx& ctx);   // device, stream and options -> ctx

@@ -107,9 +107,9 @@ static int launch_motif(MotifArgs a, LaunchCtx& ctx, int* grid_out) {
   const size_t smem = sizeof(unsigned long long) * ((a.n_classes + 1) & ~1) +
                       motif_warp_smem<W>() * MOTIF_WARPS + (a.bits_smem ? bits_bytes : 0);
   auto kern = motif_kernel<K, W>;
-  DM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  static LaunchCache cache;
   int occ = 0;
-  DM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, block, smem));
+  DM_CUDA(cached_occupancy(cache, kern, ctx.device, block, smem, &occ));
   if (occ < 1) return fail(DM_EINVAL, "motif kernel does not fit on an SM");
   int grid = ctx.num_sms * occ;
   if (ctx.threads > 0) grid = std::max(1, std::min(grid, (ctx.threads + block - 1) / block));

@@ -67,14 +67,14 @@ def make_batch(seed: int = 1, n_graphs: int = 256):
 
 def main(argv=None) -> int:
     """Runs one query on a named workload `reps` times and prints the last run's count and
-    kernel time (the command line the kernel profiles are taken with); `batch` runs the
-    batched workload instead."""
+    kernel time (the command line the kernel profiles are taken with); `upto` counts every
+    clique size 3..k in one launch; `batch` runs the batched workload instead."""
     import argparse
 
-    from . import Batch, Dictionary, count_cliques, count_motifs
+    from . import Batch, Dictionary, count_cliques, count_cliques_upto, count_motifs
 
     ap = argparse.ArgumentParser(prog="python -m dumato_b200.workloads")
-    ap.add_argument("query", choices=("clique", "motif", "batch"))
+    ap.add_argument("query", choices=("clique", "upto", "motif", "batch"))
     ap.add_argument("workload", nargs="?", default="chunglu18k", choices=sorted(CONFIGS))
     ap.add_argument("k", type=int, nargs="?", default=4)
     ap.add_argument("--reps", type=int, default=2)
@@ -91,6 +91,12 @@ def main(argv=None) -> int:
               f"(tasks {st.tasks}, donations {st.donations})")
         return 0
     g = make(args.workload, args.seed)
+    if args.query == "upto":
+        for _ in range(max(1, args.reps)):
+            counts, st = count_cliques_upto(g, args.k)
+        print(f"cliques of sizes 3..{args.k} on {args.workload}: {counts} in {st.kernel_ms:.3f} ms "
+              f"(one launch; tasks {st.tasks}, donations {st.donations})")
+        return 0
     d = Dictionary.generate(args.k) if args.query == "motif" else None
     for _ in range(max(1, args.reps)):
         if d is None:

@@ -211,6 +211,15 @@ DM_API void dm_dictionary_free(dm_dictionary* d);
 /* ---- counting (GPU only) ---- */
 /* Number of k-cliques, k in [2, 12]. */
 DM_API int dm_count_cliques(dm_graph* g, int32_t k, const dm_opts* opts, uint64_t* count, dm_stats* stats);
+/* Clique counts of every size 3..kmax (kmax in [4, 8]): counts[j] = number of (j + 3)-cliques
+   (no counterpart in the reference, whose driver counts one k per run). One launch walks the
+   clique index to depth kmax and counts every size on the way down, since a DFS to depth
+   kmax meets every smaller clique as a prefix. A graph whose index is not available, with
+   roots above 256 out-neighbours, or a call with mode DM_MODE_LIST / DM_MODE_REBUILD or a
+   subtree log, is counted with one launch per size instead (the same counts; the subtree log
+   then holds the kmax log). */
+DM_API int dm_count_cliques_upto(dm_graph* g, int32_t kmax, const dm_opts* opts, uint64_t* counts,
+                                 dm_stats* stats);
 /* Connected induced k-vertex subgraphs per class of dict (k in [3, 7]).
    class_counts has n_classes entries (dm_dictionary_shape). */
 DM_API int dm_count_motifs(dm_graph* g, int32_t k, const dm_dictionary* dict, const dm_opts* opts,

@@ -133,3 +133,39 @@ def test_live_reports_during_a_count(dm, orc, gpu):
     claimed = [s["roots_claimed"] for s in samples]
     assert claimed == sorted(claimed)
     assert [s["elapsed_ms"] for s in samples] == sorted(s["elapsed_ms"] for s in samples)
+
+
+@pytest.mark.parametrize("name", ["citeseer", "chunglu18k", "rmat100k", "rmat317k", "dense"])
+def test_fused_counts_every_size(dm, orc, gpu, name):
+    """One launch counts every clique size 3..8, each equal to the oracle's count, with and
+    without eager donation (level-0 and level-1 donations carry the fused counts too)."""
+    from dumato_b200 import workloads
+
+    if name == "citeseer":
+        g = dm.Graph.load_edgelist(GOLDEN / "citeseer.edgelist")
+    elif name == "dense":
+        g = _dense_core(dm)
+    else:
+        g = workloads.make(name, 1)
+    og = _og(orc, g)
+    want = {k: orc.clique_dag_bytes(og, k)[0] for k in range(3, 9)}
+    for flags in (0, dm.TEST_EAGER_DONATION):
+        got, st = dm.count_cliques_upto(g, 8, dm.Options(test_flags=flags))
+        assert got == want, (name, flags)
+        assert st.kernel_launches == 1
+    got6, _ = dm.count_cliques_upto(g, 6)
+    assert got6 == {k: want[k] for k in range(3, 7)}
+
+
+def test_fused_counts_fall_back_per_size(dm, orc, gpu):
+    """Where the fused walk cannot run (roots above 256 out-neighbours, list mode), the counts
+    come from one launch per size and are the same."""
+    g = _dense_core(dm, seed=9, core=300, p=0.95, n=3000, extra=20000)
+    og = _og(orc, g)
+    want = {k: orc.clique_dag_bytes(og, k)[0] for k in (3, 4)}
+    got, st = dm.count_cliques_upto(g, 4)
+    assert got == want and st.kernel_launches >= 2
+    g2 = dm.Graph.load_edgelist(GOLDEN / "citeseer.edgelist")
+    og2 = _og(orc, g2)
+    got2, _ = dm.count_cliques_upto(g2, 5, dm.Options(mode=dm.MODE_LIST))
+    assert got2 == {k: orc.clique_dag_bytes(og2, k)[0] for k in range(3, 6)}
