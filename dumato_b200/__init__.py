@@ -141,6 +141,7 @@ _SIGNATURES = {
                                                 ctypes.c_int32, ctypes.c_uint64, _P]),
     "dm_count_cliques": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.POINTER(_Opts), _P, ctypes.POINTER(_Stats)]),
     "dm_count_cliques_upto": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.POINTER(_Opts), _P, ctypes.POINTER(_Stats)]),
+    "dm_count_near_cliques": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.POINTER(_Opts), _P, ctypes.POINTER(_Stats)]),
     "dm_count_motifs": (ctypes.c_int, [_P, ctypes.c_int32, _P, ctypes.POINTER(_Opts), _P, ctypes.POINTER(_Stats)]),
     "dm_batch_create": (ctypes.c_int, [ctypes.POINTER(_Query), ctypes.c_int32, ctypes.POINTER(_Opts), ctypes.c_int32,
                                        ctypes.POINTER(_P)]),
@@ -556,6 +557,16 @@ def count_cliques_upto(g: Graph, kmax: int, opts: Optional[Options] = None) -> t
     st = _Stats()
     _check(lib().dm_count_cliques_upto(g.handle, int(kmax), ctypes.byref(o), _ptr(out), ctypes.byref(st)))
     return {k: int(out[k - 3]) for k in range(3, kmax + 1)}, Stats.from_c(st)
+
+
+def count_near_cliques(g: Graph, n: int, opts: Optional[Options] = None) -> tuple[int, Stats]:
+    """The reference's pattern-aware query q_n (n = 4..13): non-induced copies of K_n minus
+    one edge (src/main/q4_PA.cu .. q13_PA.cu)."""
+    o = (opts or Options()).to_c()
+    out = ctypes.c_uint64()
+    st = _Stats()
+    _check(lib().dm_count_near_cliques(g.handle, int(n), ctypes.byref(o), ctypes.byref(out), ctypes.byref(st)))
+    return out.value, Stats.from_c(st)
 
 
 def count_motifs(g: Graph, k: int, dictionary: Optional[Dictionary] = None,

@@ -593,6 +593,17 @@ int predictor_schedule(const void* pv, dm_graph* g, int k, bool clique, int tota
 int ensure_features(dm_graph* g, bool clique);
 void predictor_key(const void* pv, uint64_t* uid, uint64_t* version);
 
+// rank -> original id map of the DAG on the device (once per device copy)
+static int ensure_orig(dm_graph* g, DeviceSlot* s, LaunchCtx& ctx) {
+  if (s->d_orig) return DM_OK;
+  std::vector<int32_t> inv(std::max(g->n, 1));
+  for (int32_t v = 0; v < g->n; ++v) inv[g->rank[v]] = v;
+  DM_CUDA(cudaMalloc(&s->d_orig, sizeof(int32_t) * inv.size()));
+  DM_CUDA(cudaMemcpyAsync(s->d_orig, inv.data(), sizeof(int32_t) * inv.size(), cudaMemcpyHostToDevice, ctx.stream));
+  DM_CUDA(cudaStreamSynchronize(ctx.stream));
+  return DM_OK;
+}
+
 // Runs the learned schedule on the device for the input entries in_roots[0..n_in) (device
 // pointer; rank space for cliques) and points *roots / *parts (and *desc for cliques on the
 // index) at the workspace's output task list of *n entries.
@@ -608,13 +619,7 @@ static int learned_device(dm_graph* g, DeviceSlot* s, const dm_opts* o, int k, b
     DM_CUDA(cudaMalloc(&s->d_feat[eng], sizeof(float) * F.size()));
     DM_CUDA(cudaMemcpyAsync(s->d_feat[eng], F.data(), sizeof(float) * F.size(), cudaMemcpyHostToDevice, ctx.stream));
   }
-  if (clique && !s->d_orig) {
-    std::vector<int32_t> inv(std::max(g->n, 1));
-    for (int32_t v = 0; v < g->n; ++v) inv[g->rank[v]] = v;
-    DM_CUDA(cudaMalloc(&s->d_orig, sizeof(int32_t) * inv.size()));
-    DM_CUDA(cudaMemcpyAsync(s->d_orig, inv.data(), sizeof(int32_t) * inv.size(), cudaMemcpyHostToDevice, ctx.stream));
-    DM_CUDA(cudaStreamSynchronize(ctx.stream));
-  }
+  if (clique && (rc = ensure_orig(g, s, ctx))) return rc;
   const int warps = ctx.num_sms * 32;
   const int cap = learned_schedule_cap(n_in, warps);
   if ((rc = ensure_ws_bytes(reinterpret_cast<void**>(&ws.d_params), &ws.params_cap,
@@ -957,6 +962,102 @@ int dm_count_cliques_upto(dm_graph* g, int32_t kmax, const dm_opts* o, uint64_t*
     }
   }
   if (st) *st = sum;
+  return DM_OK;
+}
+
+int dm_count_near_cliques(dm_graph* g, int32_t n, const dm_opts* o, uint64_t* count, dm_stats* st) {
+  if (!g || !count) return fail(DM_EINVAL, "dm_count_near_cliques: null argument");
+  if (n < 4 || n > 13) return fail(DM_EINVAL, "dm_count_near_cliques: n must be in [4, 13]");
+  int rc = check_opts(o);
+  if (rc) return rc;
+  LaunchCtx ctx;
+  rc = select_device(o, ctx);
+  if (rc) return rc;
+  std::lock_guard<std::mutex> lk(g->mu);
+  ensure_oriented(g);
+  DeviceSlot* s = slot_for(g, ctx.device);
+  Workspace& ws = s->ws;
+  if ((rc = prepare_ws(ws, ctx.stream))) return rc;
+  DM_CUDA(cudaEventRecord(ws.ev0, ctx.stream));
+  if (!s->dg.has_oriented) {
+    rc = upload_csr(g->orow, g->oadj, g->n, g->pad_row[1], g->pad_deg[1], g->pad_adj[1], &s->dg.d_orow,
+                    &s->dg.d_odeg, &s->dg.d_oadj, ctx.stream);
+    if (rc) return rc;
+    s->dg.has_oriented = true;
+  }
+  if (!s->dg.has_undirected) {
+    rc = upload_csr(g->row, g->adj, g->n, g->pad_row[0], g->pad_deg[0], g->pad_adj[0], &s->dg.d_row, &s->dg.d_deg,
+                    &s->dg.d_adj, ctx.stream);
+    if (rc) return rc;
+    s->dg.has_undirected = true;
+  }
+  if ((rc = ensure_deg_order(g, s, ctx.stream)) || (rc = ensure_orig(g, s, ctx))) return rc;
+  const int c = n - 2;
+  const int need = c - 1;  // out-neighbours a root needs to start a c-clique
+  const int world = (o && o->world_size > 1) ? o->world_size : 1;
+  int n_roots = need <= g->max_out_degree ? (int)s->cnt_ge[need] : 0;
+  const int32_t* d_roots = s->d_deg_order;
+  if (world > 1) {
+    std::vector<int32_t> mine;
+    for (int i = o->rank; i < n_roots; i += world) mine.push_back(s->deg_order[i]);
+    if ((rc = ensure_ws_bytes(reinterpret_cast<void**>(&ws.d_tasks), &ws.tasks_cap,
+                              sizeof(int32_t) * (mine.size() + 1))))
+      return rc;
+    if (!mine.empty())
+      DM_CUDA(cudaMemcpyAsync(ws.d_tasks, mine.data(), sizeof(int32_t) * mine.size(), cudaMemcpyHostToDevice,
+                              ctx.stream));
+    d_roots = ws.d_tasks;
+    n_roots = (int)mine.size();
+  }
+  NearLaunch L;
+  L.dag = GraphView{s->dg.d_orow, s->dg.d_odeg, s->dg.d_oadj, g->n};
+  L.und = GraphView{s->dg.d_row, s->dg.d_deg, s->dg.d_adj, g->n};
+  L.orig = s->d_orig;
+  L.roots = d_roots;
+  L.n_roots = n_roots;
+  L.c = c;
+  L.ctr = ws.d_ctr;
+  L.queue = ws.d_queue;
+  L.qcap = ws.qcap;
+  L.nq = QUEUE_SHARDS;
+  L.dag_cap = g->max_out_degree + 4;
+  L.und_cap = g->max_degree + 4;
+  const size_t per_warp = near_clique_warp_ints(c, L.dag_cap, L.und_cap) * sizeof(int32_t);
+  ctx.arena_warps = (int)std::min<size_t>((size_t)ctx.num_sms * 64, std::max<size_t>(8, ((size_t)8 << 30) / per_warp));
+  if ((rc = ensure_ws_bytes(&ws.d_scratch, &ws.scratch_cap, per_warp * ctx.arena_warps))) return rc;
+  L.arena = reinterpret_cast<int32_t*>(ws.d_scratch);
+  if ((rc = init_counters(ws, n_roots, ctx.stream))) return rc;
+  DM_CUDA(cudaEventRecord(ws.k0, ctx.stream));
+  int grid = 0;
+  Reporter reporter;
+  if (n_roots > 0) {
+    if ((rc = near_clique_launch(L, ctx, &grid))) return rc;
+    if ((rc = reporter.start(o, ctx.device, ws.d_ctr, grid * 8, n_roots))) return rc;
+  }
+  DM_CUDA(cudaEventRecord(ws.k1, ctx.stream));
+  DM_CUDA(cudaMemcpyAsync(ws.h_out, ws.d_ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost, ctx.stream));
+  DM_CUDA(cudaStreamSynchronize(ctx.stream));
+  const DevCounters h = *ws.h_out;
+  if ((rc = reset_queue(ws, h, ctx.stream))) return rc;
+  float kms = 0, pms = 0;
+  cudaEventElapsedTime(&kms, ws.k0, ws.k1);
+  cudaEventElapsedTime(&pms, ws.ev0, ws.k0);
+  if (h.err) return fail(kernel_status(h.err), "near-clique kernel reported error " + std::to_string(h.err));
+  *count = h.count;
+  if (st) {
+    std::memset(st, 0, sizeof(*st));
+    st->kernel_ms = kms;
+    st->prep_ms = pms;
+    st->tasks = h.tasks;
+    st->idle_polls = h.idle_polls;
+    st->mode_used = DM_MODE_LIST;
+    st->vwarp_used = 32;
+    st->grid = grid;
+    st->block = 256;
+    st->kernel_launches = ctx.launches;
+    const double warp_ns = (double)grid * 8.0 * (double)kms * 1e6;
+    st->idle_warp_fraction = warp_ns > 0 ? std::min(1.0, (double)h.hungry_ns / warp_ns) : 0.0;
+  }
   return DM_OK;
 }
 

@@ -155,6 +155,24 @@ int clique_cached_launch(const CliqueLaunch& L, LaunchCtx& ctx, int grid);
 int clique_index_build(const GraphView& g, const int32_t* roots, int n, void* blocks, const uint32_t* boff, int m,
                        LaunchCtx& ctx);
 
+// Pattern-aware queries q4..q13 (near_clique.cu): (n-2)-cliques and their common neighbours.
+struct NearLaunch {
+  GraphView dag;                   // rank space
+  GraphView und;                   // undirected, original ids
+  const int32_t* orig = nullptr;   // rank -> original id
+  const int32_t* roots = nullptr;
+  int n_roots = 0;
+  int c = 2;                       // clique size n - 2
+  DevCounters* ctr = nullptr;
+  void* queue = nullptr;
+  int qcap = 0;
+  int nq = 1;
+  int32_t* arena = nullptr;        // near_clique_warp_ints ints per warp
+  int dag_cap = 0, und_cap = 0;
+};
+int near_clique_launch(const NearLaunch& L, LaunchCtx& ctx, int* grid);
+size_t near_clique_warp_ints(int c, int dag_cap, int und_cap);
+
 // Motif engine (motif.cu).
 struct MotifLaunch {
   GraphView g;                   // undirected CSR, original ids

@@ -220,6 +220,11 @@ DM_API int dm_count_cliques(dm_graph* g, int32_t k, const dm_opts* opts, uint64_
    then holds the kmax log). */
 DM_API int dm_count_cliques_upto(dm_graph* g, int32_t kmax, const dm_opts* opts, uint64_t* counts,
                                  dm_stats* stats);
+/* The reference's pattern-aware queries q4..q13 (src/main/q4_PA.cu .. q13_PA.cu, extension
+   steps src/main/DuMatoGPU.cu:1222-1445, run with k = n): the number of non-induced copies of
+   K_n minus one edge, n in [4, 13] - an (n-2)-clique with two vertices adjacent to all of it,
+   sum over (n-2)-cliques C of t(t-1)/2 with t the size of C's common neighbourhood. */
+DM_API int dm_count_near_cliques(dm_graph* g, int32_t n, const dm_opts* opts, uint64_t* count, dm_stats* stats);
 /* Connected induced k-vertex subgraphs per class of dict (k in [3, 7]).
    class_counts has n_classes entries (dm_dictionary_shape). */
 DM_API int dm_count_motifs(dm_graph* g, int32_t k, const dm_dictionary* dict, const dm_opts* opts,

@@ -49,6 +49,8 @@ def lib() -> ctypes.CDLL:
                                                    ctypes.c_int]),
             "oracle_motifs_brute": (ctypes.c_int, [_P, ctypes.c_int, _P, ctypes.c_int32, _P]),
             "oracle_graphlet4": (ctypes.c_int, [_P, _P, ctypes.c_int]),
+            "oracle_near_cliques": (ctypes.c_uint64, [_P, ctypes.c_int, ctypes.c_int]),
+            "oracle_near_cliques_brute": (ctypes.c_uint64, [_P, ctypes.c_int]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -207,3 +209,13 @@ def class_types4(q2c: np.ndarray, n_classes: int) -> list:
         if 0 <= c < n_classes and types[c] is None:
             types[c] = graphlet4_type(quick_edges(q, 4)) or "disconnected"
     return [None if t == "disconnected" else t for t in types]
+
+
+def near_cliques(g: OracleGraph, n: int, threads: int = 0) -> int:
+    """The reference's pattern-aware query q_n: non-induced copies of K_n minus one edge."""
+    return lib().oracle_near_cliques(g.h, n, threads)
+
+
+def near_cliques_brute(g: OracleGraph, n: int) -> int:
+    """q_n by brute force over all n-subsets (tiny graphs, n <= 8)."""
+    return lib().oracle_near_cliques_brute(g.h, n)

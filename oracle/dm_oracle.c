@@ -763,3 +763,115 @@ int oracle_graphlet4(const og_graph *g, uint64_t *out, int threads) {
   out[5] = Q;
   return 0;
 }
+
+/* ---------------- pattern-aware queries q4..q13 ----------------
+   src/main/q{n}_PA.cu with the extension steps of src/main/DuMatoGPU.cu:1222-1445, run with
+   k = n: an increasing (n-2)-clique v_0 < .. < v_{n-3} (extend_single above v_0, then
+   intersect with N(v_l) above v_l), then v_{n-2} from the clique's common neighbourhood
+   outside the prefix (extend_single + intersect_unique) and v_{n-1} from the same set above
+   v_{n-2} (copy_extensions), counted at the last level. The count is therefore the sum over
+   (n-2)-cliques of t(t-1)/2, t = |common neighbourhood| (members excluded, self-loops
+   ignored). Cliques come from the degree-ordered DAG, one per vertex set. */
+static uint64_t near_root(const og_graph *g, const og_dag *d, int32_t r, int c, int32_t *buf, int32_t cap,
+                          int32_t *mem, int32_t *sc0, int32_t *sc1) {
+  int32_t *C[16];
+  int32_t nC[16], pos[16];
+  uint64_t total = 0;
+  mem[0] = d->orig[r];
+  C[0] = buf;
+  nC[0] = (int32_t)(d->off[r + 1] - d->off[r]);
+  memcpy(C[0], d->adj + d->off[r], sizeof(int32_t) * nC[0]);
+  for (int i = 1; i < c; ++i) C[i] = buf + (size_t)i * cap;
+  int l = 0;
+  pos[0] = 0;
+  if (c == 1) l = -1;
+  while (l >= 0) {
+    if (pos[l] >= nC[l]) {
+      --l;
+      continue;
+    }
+    int32_t v = C[l][pos[l]++];
+    mem[l + 1] = d->orig[v];
+    if (l + 2 == c) {
+      /* common neighbourhood of mem[0..c) in the undirected graph */
+      int32_t n = 0;
+      const int32_t u0 = mem[0];
+      for (int64_t e = g->off[u0]; e < g->off[u0 + 1]; ++e) sc0[n++] = g->adj[e];
+      for (int i = 1; i < c && n; ++i) {
+        const int32_t u = mem[i];
+        n = intersect_sorted(sc0, n, g->adj + g->off[u], (int32_t)(g->off[u + 1] - g->off[u]), sc1);
+        memcpy(sc0, sc1, sizeof(int32_t) * (size_t)n);
+      }
+      uint64_t t = 0;
+      for (int32_t j = 0; j < n; ++j) {
+        int member = 0;
+        for (int i = 0; i < c; ++i) member |= sc0[j] == mem[i];
+        t += !member;
+      }
+      total += t * (t > 0 ? t - 1 : 0) / 2;
+      continue;
+    }
+    int32_t nv = (int32_t)(d->off[v + 1] - d->off[v]);
+    nC[l + 1] = intersect_sorted(C[l] + pos[l], nC[l] - pos[l], d->adj + d->off[v], nv, C[l + 1]);
+    ++l;
+    pos[l] = 0;
+  }
+  return total;
+}
+
+uint64_t oracle_near_cliques(const og_graph *g, int n, int threads) {
+  if (n < 4 || n > 13) return 0;
+  const int c = n - 2;
+  og_dag *d = make_dag(g);
+  int32_t maxo = 0;
+  for (int32_t r = 0; r < d->n; ++r) {
+    int32_t x = (int32_t)(d->off[r + 1] - d->off[r]);
+    if (x > maxo) maxo = x;
+  }
+  const int32_t cap = maxo + 1, ucap = g->maxdeg + 1;
+  uint64_t total = 0;
+#pragma omp parallel num_threads(resolve_threads(threads)) reduction(+ : total)
+  {
+    int32_t *buf = (int32_t *)malloc(sizeof(int32_t) * (size_t)cap * (c + 1));
+    int32_t *sc0 = (int32_t *)malloc(sizeof(int32_t) * (size_t)ucap);
+    int32_t *sc1 = (int32_t *)malloc(sizeof(int32_t) * (size_t)ucap);
+    int32_t mem[16];
+#pragma omp for schedule(dynamic, 16)
+    for (int32_t r = 0; r < d->n; ++r) total += near_root(g, d, r, c, buf, cap, mem, sc0, sc1);
+    free(buf);
+    free(sc0);
+    free(sc1);
+  }
+  free_dag(d);
+  return total;
+}
+
+/* The same count by brute force over all n-subsets and all choices of the missing pair (tiny
+   graphs only): non-induced copies of K_n minus one edge. */
+uint64_t oracle_near_cliques_brute(const og_graph *g, int n) {
+  if (n < 4 || n > 8 || g->n > 40) return 0;
+  int32_t s[8];
+  uint64_t total = 0;
+  for (int i = 0; i < n; ++i) s[i] = i;
+  while (1) {
+    if (s[n - 1] < g->n) {
+      /* each unordered pair (a, b) may be the missing edge; all other pairs must be edges */
+      for (int a = 0; a < n; ++a)
+        for (int b = a + 1; b < n; ++b) {
+          int ok = 1;
+          for (int x = 0; x < n && ok; ++x)
+            for (int y = x + 1; y < n && ok; ++y) {
+              if (x == a && y == b) continue;
+              if (!bin_find(g, s[x], s[y]) || s[x] == s[y]) ok = 0;
+            }
+          total += ok;
+        }
+    }
+    int i = n - 1;
+    while (i >= 0 && s[i] == g->n - n + i) --i;
+    if (i < 0) break;
+    ++s[i];
+    for (int j = i + 1; j < n; ++j) s[j] = s[j - 1] + 1;
+  }
+  return total;
+}

@@ -14,13 +14,16 @@ small R-MAT graph (ids < 2,000, 8,000 edges, seed 3; motifs up to k = 4 there, s
 (~321k vertices, 1.05M edges; 7-cliques). Runs use the reference's recommended launch shape
 (102400 threads, 256 per block, 16 donations) with threshold 100 (no balancing), plus
 threshold-30 runs (host-mediated balancing on) on citeseer (k = 4) and on the Chung-Lu
-graph (k = 4..7).
+graph (k = 4..7), and the pattern-aware queries q4..q13 (`q<n>_PA` run with k = n) on the
+small graphs.
 
 A run is only made where the reference's per-warp extension buffers provably hold every
 write. Motifs: each level's buffer is nextpow2(l * max(32, dmax)) ints and a level's writes
 reach index <= (l-1)*dmax + roundup32(dmax) - 1 (DuMatoCPU.cu:70-87, DuMatoGPU.cu:317-343).
-Cliques (pattern-aware buffers of nextpow2(max(32, dmax)) ints per level): extend_clique
-writes at most roundup32(degree) <= that many entries (DuMatoGPU.cu:1194-1220), on any graph.
+Cliques and the q_n queries (pattern-aware buffers of nextpow2(max(32, dmax)) ints per
+level): extend_clique, extend_single, intersect, intersect_unique and copy_extensions write at
+most roundup32(size of the list they filter) <= that many entries (DuMatoGPU.cu:1028-1075,
+353-434, 1194-1445), on any graph.
 """
 from __future__ import annotations
 
@@ -85,6 +88,8 @@ def main(out_path: str, only: set | None) -> None:
     clique_ks = {"chunglu18k_s1": (4, 5, 6, 7), "rmat317k_s1": (7,)}
     motif_ks = {"rmat2k_s3": (3, 4), "chunglu18k_s1": (3, 4), "rmat317k_s1": ()}
     lb_runs = {"citeseer": (4,), "chunglu18k_s1": (4, 5, 6, 7)}
+    # pattern-aware queries q_n (run with k = n), on the small graphs
+    near_ns = {"test": range(4, 8), "citeseer": range(4, 14), "er2k_s1": range(4, 8), "rmat2k_s3": range(4, 10)}
     out = json.loads(Path(out_path).read_text()) if Path(out_path).exists() else {}
     for name, path in graphs.items():
         if only and name not in only:
@@ -105,6 +110,12 @@ def main(out_path: str, only: set | None) -> None:
             total = int(re.search(r"Aggregated: (\d+),", txt).group(1))
             entry["motifs"][str(k)] = {"classes": counts, "total": total}
             entry["time_gpu_s"][f"motifs{k}"] = float(re.search(r"Time \(GPU\): ([0-9.]+)", txt).group(1))
+        if name in near_ns:
+            entry["near"] = {}
+            for q in near_ns[name]:
+                txt = run(f"q{q}_PA", path, q, 100, timeout=600)
+                entry["near"][str(q)] = int(re.search(r"Result: (\d+)\.", txt).group(1))
+                entry["time_gpu_s"][f"q{q}"] = float(re.search(r"Time \(GPU\): ([0-9.]+)", txt).group(1))
         if name in lb_runs:
             entry["clique_lb_threshold30"] = {}
             for k in lb_runs[name]:

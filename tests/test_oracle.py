@@ -95,6 +95,8 @@ def test_oracle_matches_reference_binaries(dm, orc):
                 assert got == c, (name, key, k)
         for k, mot in entry["motifs"].items():
             assert _ref_motif_check(orc, g, int(k), mot, large), (name, k)
+        for q, c in entry.get("near", {}).items():
+            assert orc.near_cliques(g, int(q)) == c, (name, "q", q)
 
 
 def _by_type(orc, dm, og):
@@ -139,3 +141,22 @@ def test_class_types_of_the_reference_dictionary(dm, orc):
     conn = d.connected()
     assert sorted(t for t, c in zip(types, conn) if c) == sorted(orc.GRAPHLET4_TYPES)
     assert all(t is None for t, c in zip(types, conn) if not c)
+
+
+@pytest.mark.parametrize("seed", range(4))
+def test_near_cliques_match_brute_force(orc, seed):
+    """q_n (K_n minus one edge, non-induced) from the (n-2)-clique formula equals brute force."""
+    rng = np.random.default_rng(200 + seed)
+    n = int(rng.integers(10, 16))
+    m = int(rng.integers(2 * n, n * (n - 1) // 2))
+    s, t = rng.integers(0, n, m), rng.integers(0, n, m)
+    g = orc.OracleGraph.from_pairs(s, t)
+    for q in (4, 5, 6):
+        assert orc.near_cliques(g, q) == orc.near_cliques_brute(g, q), q
+
+
+def test_q4_is_the_diamond_subgraph_count(orc):
+    """q4 counts non-induced diamonds: the closed-form checker's diamond + 6 x 4-clique total."""
+    g = orc.OracleGraph.load(GOLDEN / "citeseer.edgelist")
+    gl = orc.graphlet4(g)
+    assert orc.near_cliques(g, 4) == gl["diamond"] + 6 * gl["clique"]
