@@ -18,7 +18,7 @@ def run(args, cwd=None):
     return subprocess.run([str(a) for a in args], capture_output=True, text=True, cwd=cwd, timeout=600)
 
 
-@pytest.mark.parametrize("exe", ["clique", "motifs"])
+@pytest.mark.parametrize("exe", ["clique", "motifs", "near_clique"])
 def test_wrong_argument_count(dm, exe):
     r = run([BIN / exe, GOLDEN / "test.edgelist", 3])
     assert r.returncode == 1 and "Wrong amount of parameters!" in r.stdout
@@ -66,3 +66,13 @@ def test_motifs_without_dictionary_file_generates_one(dm, gpu, tmp_path):
     r = run([BIN / "motifs", GOLDEN / "test.edgelist", 4, 0, 256, 16, 30], cwd=tmp_path)
     assert r.returncode == 0, r.stderr
     assert "Aggregated: 4, 3 patterns." in r.stdout
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("q", [4, 5, 6])
+def test_near_clique_result_line(dm, orc, gpu, q):
+    """`near_clique graph k ...` prints the count of the reference's q<k>_PA."""
+    r = run([BIN / "near_clique", GOLDEN / "citeseer.edgelist", q, 102400, 256, 16, 30])
+    assert r.returncode == 0, r.stderr
+    og = orc.OracleGraph.load(GOLDEN / "citeseer.edgelist")
+    assert f"Result: {orc.near_cliques(og, q)}." in r.stdout
