@@ -65,6 +65,16 @@ struct dm_graph {
   // padded device layout of the CSRs (0: undirected, 1: degree-ordered DAG), built on the
   // first upload and kept, so uploading the graph again is a plain copy
   std::vector<int32_t> pad_row[2], pad_deg[2], pad_adj[2];
+  // device-independent task orders and clique-index layout, computed once and kept with the
+  // graph for the same reason
+  std::vector<int32_t> deg_order;     // ranks by descending DAG out-degree (stable in rank)
+  std::vector<int64_t> cnt_ge;        // cnt_ge[d] = ranks with out-degree >= d
+  std::vector<uint32_t> idx_boff;     // clique-index block offset per rank (16-byte units)
+  std::vector<int32_t> idx_desc;      // task list of deg_order on the index, 4 ints per entry
+  uint64_t idx_units = 0;             // 16-byte units of the whole index
+  int32_t idx_maxd = 0;               // largest out-degree with a block
+  std::vector<int32_t> up_order;      // motif roots by descending upper degree
+  std::vector<void*> pinned;          // host arrays registered with the CUDA driver
   // device copies
   std::mutex mu;
   std::vector<dmb::DeviceGraph*> dev;
@@ -87,4 +97,5 @@ int build_graph_from_pairs(std::vector<uint64_t>& keys, int32_t n_vertices, int6
 void ensure_oriented(dm_graph* g);
 // device helpers (engine.cu)
 void release_device_graphs(dm_graph* g);
+void unpin_host_arrays(dm_graph* g);
 }  // namespace dmb

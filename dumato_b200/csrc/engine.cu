@@ -101,8 +101,6 @@ struct DeviceSlot {
   // roots (rank space) in descending out-degree order, resident on the device; the roots
   // eligible for k-cliques (out-degree >= k-1) are a prefix of it
   int32_t* d_deg_order = nullptr;
-  std::vector<int32_t> deg_order;
-  std::vector<int64_t> cnt_ge;  // cnt_ge[d] = roots with out-degree >= d
   // motif roots (vertices with a neighbour above them) by descending upper degree
   int32_t* d_up_order = nullptr;
   int n_up = 0;
@@ -111,7 +109,6 @@ struct DeviceSlot {
   int index_state = 0;              // 0 not built, 1 built, -1 over the memory budget
   void* d_blocks = nullptr;
   uint32_t* d_boff = nullptr;
-  std::vector<uint32_t> boff;       // host copy, rank space
   size_t index_bytes = 0;
   RootDesc* d_desc_deg = nullptr;   // task list of the descending-degree order (index counting)
   // learned scheduler inputs on the device: base features per engine (0 = motifs, 1 =
@@ -337,9 +334,69 @@ static DeviceSlot* slot_for(dm_graph* g, int dev) {
   return s;
 }
 
+// Device buffers owned by graphs (CSR copies, root orders, the clique index) go back to a
+// per-device pool when a graph's device copy is released, and the next upload of the same
+// or another graph takes them from there (best fit, at most twice the size asked for), so
+// re-uploading a graph costs copies, not cudaMalloc/cudaFree. The pool holds at most 4 GB.
+static std::mutex g_buf_mu;
+static std::map<void*, size_t> g_buf_size;
+static std::map<int, std::multimap<size_t, void*>> g_buf_pool;
+static size_t g_buf_pooled = 0;
+constexpr size_t BUF_POOL_MAX = (size_t)4 << 30;
+
+static cudaError_t gbuf_alloc(void** p, size_t bytes) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  bytes = (std::max<size_t>(bytes, 256) + 255) / 256 * 256;
+  std::lock_guard<std::mutex> lk(g_buf_mu);
+  auto& pool = g_buf_pool[dev];
+  auto it = pool.lower_bound(bytes);
+  if (it != pool.end() && it->first <= 2 * bytes) {
+    *p = it->second;
+    g_buf_pooled -= it->first;
+    pool.erase(it);
+    return cudaSuccess;
+  }
+  e = cudaMalloc(p, bytes);
+  if (e == cudaSuccess) g_buf_size[*p] = bytes;
+  return e;
+}
+
+static void gbuf_free(void* p, int dev) {
+  if (!p) return;
+  std::lock_guard<std::mutex> lk(g_buf_mu);
+  auto it = g_buf_size.find(p);
+  if (it != g_buf_size.end() && g_buf_pooled + it->second <= BUF_POOL_MAX) {
+    g_buf_pool[dev].insert({it->second, p});
+    g_buf_pooled += it->second;
+    return;
+  }
+  if (it != g_buf_size.end()) g_buf_size.erase(it);
+  cudaFree(p);
+}
+
+// Registers a host array of the graph with the driver once (page-locked), so uploads from it
+// are asynchronous DMA; the arrays are never resized afterwards and are unregistered when the
+// graph is freed.
+static void pin_host(dm_graph* g, const void* p, size_t bytes) {
+  if (!p || !bytes) return;
+  if (std::find(g->pinned.begin(), g->pinned.end(), p) != g->pinned.end()) return;
+  if (cudaHostRegister(const_cast<void*>(p), bytes, cudaHostRegisterPortable) == cudaSuccess)
+    g->pinned.push_back(const_cast<void*>(p));
+  else
+    cudaGetLastError();
+}
+
+void unpin_host_arrays(dm_graph* g) {
+  for (void* p : g->pinned) cudaHostUnregister(p);
+  g->pinned.clear();
+  cudaGetLastError();
+}
+
 // Pads rows to multiples of 4 ints (16 bytes) filled with INT32_MAX; the padded layout is
-// built on the first upload of a graph and kept with it.
-static int upload_csr(const std::vector<int64_t>& row, const std::vector<int32_t>& adj, int32_t n,
+// built on the first upload of a graph and kept (page-locked) with it.
+static int upload_csr(dm_graph* g, const std::vector<int64_t>& row, const std::vector<int32_t>& adj, int32_t n,
                       std::vector<int32_t>& prow, std::vector<int32_t>& pdeg, std::vector<int32_t>& padj,
                       int32_t** d_row, int32_t** d_deg, int32_t** d_adj, cudaStream_t st) {
   if (padj.empty()) {
@@ -359,21 +416,26 @@ static int upload_csr(const std::vector<int64_t>& row, const std::vector<int32_t
     }
     padj.assign((size_t)std::max<int64_t>(total, 4), INT32_MAX);
     for (int32_t v = 0; v < n; ++v) std::memcpy(padj.data() + prow[v], adj.data() + row[v], sizeof(int32_t) * pdeg[v]);
+    pin_host(g, prow.data(), sizeof(int32_t) * prow.size());
+    pin_host(g, pdeg.data(), sizeof(int32_t) * pdeg.size());
+    pin_host(g, padj.data(), sizeof(int32_t) * padj.size());
   }
   // the three buffers are published together: a failure frees what was allocated
   int32_t *r = nullptr, *d = nullptr, *a = nullptr;
-  cudaError_t e = cudaMalloc(&r, sizeof(int32_t) * std::max(n, 1));
-  if (e == cudaSuccess) e = cudaMalloc(&d, sizeof(int32_t) * std::max(n, 1));
-  if (e == cudaSuccess) e = cudaMalloc(&a, sizeof(int32_t) * padj.size());
+  int dev = 0;
+  cudaGetDevice(&dev);
+  cudaError_t e = gbuf_alloc(reinterpret_cast<void**>(&r), sizeof(int32_t) * std::max(n, 1));
+  if (e == cudaSuccess) e = gbuf_alloc(reinterpret_cast<void**>(&d), sizeof(int32_t) * std::max(n, 1));
+  if (e == cudaSuccess) e = gbuf_alloc(reinterpret_cast<void**>(&a), sizeof(int32_t) * padj.size());
   if (e == cudaSuccess && n) e = cudaMemcpyAsync(r, prow.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess && n) e = cudaMemcpyAsync(d, pdeg.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(a, padj.data(), sizeof(int32_t) * padj.size(), cudaMemcpyHostToDevice, st);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  // (the host arrays live as long as the graph: no synchronisation is needed here)
   if (e != cudaSuccess) {
-    cudaFree(r);
-    cudaFree(d);
-    cudaFree(a);
+    gbuf_free(r, dev);
+    gbuf_free(d, dev);
+    gbuf_free(a, dev);
     return fail(e == cudaErrorMemoryAllocation ? DM_ENOMEM : DM_ECUDA,
                 std::string("graph upload failed: ") + cudaGetErrorString(e));
   }
@@ -439,12 +501,12 @@ void release_device_graphs(dm_graph* g) {
     int cur = 0;
     if (cudaGetDevice(&cur) == cudaSuccess) {
       cudaSetDevice(s->dg.device);
-      cudaFree(s->dg.d_row);
-      cudaFree(s->dg.d_deg);
-      cudaFree(s->dg.d_adj);
-      cudaFree(s->dg.d_orow);
-      cudaFree(s->dg.d_odeg);
-      cudaFree(s->dg.d_oadj);
+      const int dv = s->dg.device;
+      for (void* p : {(void*)s->dg.d_row, (void*)s->dg.d_deg, (void*)s->dg.d_adj, (void*)s->dg.d_orow,
+                      (void*)s->dg.d_odeg, (void*)s->dg.d_oadj, (void*)s->d_deg_order, (void*)s->d_up_order,
+                      s->d_blocks, (void*)s->d_boff, (void*)s->d_desc_deg, (void*)s->d_feat[0], (void*)s->d_feat[1],
+                      (void*)s->d_orig})
+        gbuf_free(p, dv);
       {
         std::lock_guard<std::mutex> lk(g_dev_mu);
         auto& pool = g_ws_pool[s->dg.device];
@@ -454,14 +516,7 @@ void release_device_graphs(dm_graph* g) {
         }
       }
       free_workspace(s->ws);
-      cudaFree(s->d_deg_order);
-      cudaFree(s->d_up_order);
-      cudaFree(s->d_blocks);
-      cudaFree(s->d_boff);
-      cudaFree(s->d_desc_deg);
-      cudaFree(s->d_feat[0]);
-      cudaFree(s->d_feat[1]);
-      cudaFree(s->d_orig);
+
       cudaSetDevice(cur);
     }
     cudaGetLastError();
@@ -498,28 +553,33 @@ int check_opts(const dm_opts* o) {
   return DM_OK;
 }
 
-// Descending out-degree order of all roots, uploaded once per (graph, device).
+// Descending out-degree order of all roots: computed once per graph (host), uploaded once
+// per device copy.
 static int ensure_deg_order(dm_graph* g, DeviceSlot* s, cudaStream_t st) {
   if (s->d_deg_order) return DM_OK;
   const int32_t n = g->n;
-  const int maxd = g->max_out_degree;
-  std::vector<int64_t> cnt((size_t)maxd + 2, 0);
-  for (int32_t r = 0; r < n; ++r) cnt[g->orow[r + 1] - g->orow[r]]++;
-  s->cnt_ge.assign((size_t)maxd + 2, 0);
-  for (int d = maxd; d >= 0; --d) s->cnt_ge[d] = s->cnt_ge[d + 1] + cnt[d];
-  // counting sort by descending degree, stable in rank
-  std::vector<int64_t> pos((size_t)maxd + 2, 0);
-  for (int d = 0; d <= maxd; ++d) pos[d] = s->cnt_ge[d + 1];
-  s->deg_order.assign(n, 0);
-  for (int32_t r = 0; r < n; ++r) s->deg_order[pos[g->orow[r + 1] - g->orow[r]]++] = r;
-  DM_CUDA(cudaMalloc(&s->d_deg_order, sizeof(int32_t) * std::max(n, 1)));
+  if (g->deg_order.size() != (size_t)n || g->cnt_ge.empty()) {
+    const int maxd = g->max_out_degree;
+    std::vector<int64_t> cnt((size_t)maxd + 2, 0);
+    for (int32_t r = 0; r < n; ++r) cnt[g->orow[r + 1] - g->orow[r]]++;
+    g->cnt_ge.assign((size_t)maxd + 2, 0);
+    for (int d = maxd; d >= 0; --d) g->cnt_ge[d] = g->cnt_ge[d + 1] + cnt[d];
+    // counting sort by descending degree, stable in rank
+    std::vector<int64_t> pos((size_t)maxd + 2, 0);
+    for (int d = 0; d <= maxd; ++d) pos[d] = g->cnt_ge[d + 1];
+    g->deg_order.assign(n, 0);
+    for (int32_t r = 0; r < n; ++r) g->deg_order[pos[g->orow[r + 1] - g->orow[r]]++] = r;
+    pin_host(g, g->deg_order.data(), sizeof(int32_t) * g->deg_order.size());
+  }
+  DM_CUDA(gbuf_alloc(reinterpret_cast<void**>(&s->d_deg_order), sizeof(int32_t) * std::max(n, 1)));
   if (n)
-    DM_CUDA(cudaMemcpyAsync(s->d_deg_order, s->deg_order.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, st));
+    DM_CUDA(cudaMemcpyAsync(s->d_deg_order, g->deg_order.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, st));
   return DM_OK;
 }
 
-static RootDesc root_desc(const dm_graph* g, const DeviceSlot* s, int32_t r, int32_t part) {
-  return RootDesc{r, (int32_t)(g->orow[r + 1] - g->orow[r]), s->boff.empty() ? INDEX_NONE : s->boff[r], part};
+static RootDesc root_desc(const dm_graph* g, const DeviceSlot* /*s*/, int32_t r, int32_t part) {
+  return RootDesc{r, (int32_t)(g->orow[r + 1] - g->orow[r]), g->idx_boff.empty() ? INDEX_NONE : g->idx_boff[r],
+                  part};
 }
 
 // Builds the clique index of this device copy (once): host block offsets, the device
@@ -529,60 +589,71 @@ static RootDesc root_desc(const dm_graph* g, const DeviceSlot* s, int32_t r, int
 static int ensure_index(dm_graph* g, DeviceSlot* s, LaunchCtx& ctx) {
   if (s->index_state != 0) return DM_OK;
   const int32_t n = g->n;
-  std::vector<uint32_t> boff((size_t)n, INDEX_NONE);
-  uint64_t total = 0;
-  int max_d = 0;
-  for (int32_t r = 0; r < n; ++r) {
-    const int d = (int)(g->orow[r + 1] - g->orow[r]);
-    if (d >= 2 && d <= INDEX_MAX_DEGREE) {
-      boff[r] = (uint32_t)total;
-      total += index_block_units_host(d);
-      max_d = std::max(max_d, d);
+  if (g->idx_boff.size() != (size_t)n) {
+    // block offsets and the task list of the descending-degree order, once per graph
+    std::vector<uint32_t> boff((size_t)n, INDEX_NONE);
+    uint64_t total = 0;
+    int max_d = 0;
+    for (int32_t r = 0; r < n; ++r) {
+      const int d = (int)(g->orow[r + 1] - g->orow[r]);
+      if (d >= 2 && d <= INDEX_MAX_DEGREE) {
+        boff[r] = total < INDEX_NONE ? (uint32_t)total : INDEX_NONE;
+        total += index_block_units_host(d);
+        max_d = std::max(max_d, d);
+      }
     }
+    g->idx_boff.swap(boff);
+    g->idx_units = total;
+    g->idx_maxd = max_d;
+    g->idx_desc.assign((size_t)4 * n, 0);
+    for (int32_t i = 0; i < n; ++i) {
+      const RootDesc rd = root_desc(g, s, g->deg_order[i], 0);
+      std::memcpy(g->idx_desc.data() + 4 * (size_t)i, &rd, sizeof(RootDesc));
+    }
+    pin_host(g, g->idx_boff.data(), sizeof(uint32_t) * g->idx_boff.size());
+    pin_host(g, g->idx_desc.data(), sizeof(int32_t) * g->idx_desc.size());
   }
-  size_t free_b = 0, tot_b = 0;
-  DM_CUDA(cudaMemGetInfo(&free_b, &tot_b));
+  const uint64_t total = g->idx_units;
   const size_t bytes = (size_t)total * 16;
-  if (total >= INDEX_NONE || bytes > std::min<size_t>((size_t)8 << 30, free_b / 4)) {
+  bool fits = total < INDEX_NONE;
+  if (fits && bytes > ((size_t)256 << 20)) {
+    size_t free_b = 0, tot_b = 0;
+    DM_CUDA(cudaMemGetInfo(&free_b, &tot_b));
+    fits = bytes <= std::min<size_t>((size_t)8 << 30, free_b / 4);
+  }
+  if (!fits) {
     s->index_state = -1;
     return DM_OK;
   }
   void* blocks = nullptr;
   uint32_t* d_boff = nullptr;
   RootDesc* desc = nullptr;
-  cudaError_t e = cudaMalloc(&blocks, std::max<size_t>(bytes, 16));
-  if (e == cudaSuccess) e = cudaMalloc(&d_boff, sizeof(uint32_t) * std::max(n, 1));
-  if (e == cudaSuccess) e = cudaMalloc(&desc, sizeof(RootDesc) * std::max(n, 1));
+  cudaError_t e = gbuf_alloc(&blocks, std::max<size_t>(bytes, 16));
+  if (e == cudaSuccess) e = gbuf_alloc(reinterpret_cast<void**>(&d_boff), sizeof(uint32_t) * std::max(n, 1));
+  if (e == cudaSuccess) e = gbuf_alloc(reinterpret_cast<void**>(&desc), sizeof(RootDesc) * std::max(n, 1));
   if (e != cudaSuccess) {
-    cudaFree(blocks);
-    cudaFree(d_boff);
-    cudaFree(desc);
+    gbuf_free(blocks, ctx.device);
+    gbuf_free(d_boff, ctx.device);
+    gbuf_free(desc, ctx.device);
     cudaGetLastError();
     s->index_state = -1;  // no room: per-launch bitmaps
     return DM_OK;
   }
-  s->boff.swap(boff);
-  std::vector<RootDesc> hd((size_t)n);
-  for (int32_t i = 0; i < n; ++i) hd[i] = root_desc(g, s, s->deg_order[i], 0);
   s->d_blocks = blocks;
   s->d_boff = d_boff;
   s->d_desc_deg = desc;
   s->index_bytes = bytes;
   s->index_state = 1;
   if (n) {
-    DM_CUDA(cudaMemcpyAsync(d_boff, s->boff.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice, ctx.stream));
-    DM_CUDA(cudaMemcpyAsync(desc, hd.data(), sizeof(RootDesc) * n, cudaMemcpyHostToDevice, ctx.stream));
+    DM_CUDA(cudaMemcpyAsync(d_boff, g->idx_boff.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice, ctx.stream));
+    DM_CUDA(cudaMemcpyAsync(desc, g->idx_desc.data(), sizeof(RootDesc) * n, cudaMemcpyHostToDevice, ctx.stream));
   }
   // roots with out-degree in [2, 256] are a contiguous range of the descending-degree order
-  const int64_t lo = INDEX_MAX_DEGREE + 1 < (int64_t)s->cnt_ge.size() ? s->cnt_ge[INDEX_MAX_DEGREE + 1] : 0;
-  const int64_t hi = 2 < (int64_t)s->cnt_ge.size() ? s->cnt_ge[2] : 0;
+  const int64_t lo = INDEX_MAX_DEGREE + 1 < (int64_t)g->cnt_ge.size() ? g->cnt_ge[INDEX_MAX_DEGREE + 1] : 0;
+  const int64_t hi = 2 < (int64_t)g->cnt_ge.size() ? g->cnt_ge[2] : 0;
   const GraphView gv{s->dg.d_orow, s->dg.d_odeg, s->dg.d_oadj, n};
-  int rc = clique_index_build(gv, s->d_deg_order + lo, (int)(hi - lo), blocks, d_boff,
-                              std::max(1, (std::min(INDEX_MAX_DEGREE, max_d) + 63) / 64), ctx);
-  if (rc) return rc;
-  // the host vector must outlive the asynchronous copy
-  DM_CUDA(cudaStreamSynchronize(ctx.stream));
-  return DM_OK;
+  return clique_index_build(gv, s->d_deg_order + lo, (int)(hi - lo), blocks, d_boff,
+                            std::max(1, (std::min(INDEX_MAX_DEGREE, g->idx_maxd) + 63) / 64), ctx);
 }
 
 // Root order (shared by both engines): plain = descending degree (heaviest first), id =
@@ -598,7 +669,7 @@ static int ensure_orig(dm_graph* g, DeviceSlot* s, LaunchCtx& ctx) {
   if (s->d_orig) return DM_OK;
   std::vector<int32_t> inv(std::max(g->n, 1));
   for (int32_t v = 0; v < g->n; ++v) inv[g->rank[v]] = v;
-  DM_CUDA(cudaMalloc(&s->d_orig, sizeof(int32_t) * inv.size()));
+  DM_CUDA(gbuf_alloc(reinterpret_cast<void**>(&s->d_orig), sizeof(int32_t) * inv.size()));
   DM_CUDA(cudaMemcpyAsync(s->d_orig, inv.data(), sizeof(int32_t) * inv.size(), cudaMemcpyHostToDevice, ctx.stream));
   DM_CUDA(cudaStreamSynchronize(ctx.stream));
   return DM_OK;
@@ -616,7 +687,7 @@ static int learned_device(dm_graph* g, DeviceSlot* s, const dm_opts* o, int k, b
   if (!s->d_feat[eng]) {
     const auto& F = g->feat[eng];
     if (F.empty()) return fail(DM_EINVAL, "predictor features were not prepared");
-    DM_CUDA(cudaMalloc(&s->d_feat[eng], sizeof(float) * F.size()));
+    DM_CUDA(gbuf_alloc(reinterpret_cast<void**>(&s->d_feat[eng]), sizeof(float) * F.size()));
     DM_CUDA(cudaMemcpyAsync(s->d_feat[eng], F.data(), sizeof(float) * F.size(), cudaMemcpyHostToDevice, ctx.stream));
   }
   if (clique && (rc = ensure_orig(g, s, ctx))) return rc;
@@ -734,7 +805,7 @@ static int count_cliques_impl(dm_graph* g, int32_t k, const dm_opts* o, uint64_t
   if ((rc = prepare_ws(ws, ctx.stream))) return rc;
   DM_CUDA(cudaEventRecord(ws.ev0, ctx.stream));
   if (!s->dg.has_oriented) {
-    rc = upload_csr(g->orow, g->oadj, g->n, g->pad_row[1], g->pad_deg[1], g->pad_adj[1], &s->dg.d_orow,
+    rc = upload_csr(g, g->orow, g->oadj, g->n, g->pad_row[1], g->pad_deg[1], g->pad_adj[1], &s->dg.d_orow,
                     &s->dg.d_odeg, &s->dg.d_oadj, ctx.stream);
     if (rc) return rc;
     s->dg.has_oriented = true;
@@ -753,18 +824,18 @@ static int count_cliques_impl(dm_graph* g, int32_t k, const dm_opts* o, uint64_t
   int n_roots = 0, max_d = 0;
   if (sched == DM_SCHED_PLAIN && world == 1) {
     // the eligible roots are a prefix of the cached descending-degree order
-    n_roots = need <= g->max_out_degree ? (int)s->cnt_ge[need] : 0;
+    n_roots = need <= g->max_out_degree ? (int)g->cnt_ge[need] : 0;
     d_roots = s->d_deg_order;
     d_desc = s->d_desc_deg;
-    max_d = n_roots ? (int)(g->orow[s->deg_order[0] + 1] - g->orow[s->deg_order[0]]) : 0;
+    max_d = n_roots ? (int)(g->orow[g->deg_order[0] + 1] - g->orow[g->deg_order[0]]) : 0;
   }
   const int32_t* d_parts = nullptr;
   if (d_roots) {
   } else if (sched == DM_SCHED_LEARNED) {
     // the plain order (this shard of it), reordered and split by the schedule on the device
     const int32_t* in = s->d_deg_order;
-    int n_in = need <= g->max_out_degree ? (int)s->cnt_ge[need] : 0;
-    if (n_in) max_d = (int)(g->orow[s->deg_order[0] + 1] - g->orow[s->deg_order[0]]);
+    int n_in = need <= g->max_out_degree ? (int)g->cnt_ge[need] : 0;
+    if (n_in) max_d = (int)(g->orow[g->deg_order[0] + 1] - g->orow[g->deg_order[0]]);
     if (world > 1) {
       dm_opts po = *o;
       po.scheduler = DM_SCHED_PLAIN;
@@ -980,13 +1051,13 @@ int dm_count_near_cliques(dm_graph* g, int32_t n, const dm_opts* o, uint64_t* co
   if ((rc = prepare_ws(ws, ctx.stream))) return rc;
   DM_CUDA(cudaEventRecord(ws.ev0, ctx.stream));
   if (!s->dg.has_oriented) {
-    rc = upload_csr(g->orow, g->oadj, g->n, g->pad_row[1], g->pad_deg[1], g->pad_adj[1], &s->dg.d_orow,
+    rc = upload_csr(g, g->orow, g->oadj, g->n, g->pad_row[1], g->pad_deg[1], g->pad_adj[1], &s->dg.d_orow,
                     &s->dg.d_odeg, &s->dg.d_oadj, ctx.stream);
     if (rc) return rc;
     s->dg.has_oriented = true;
   }
   if (!s->dg.has_undirected) {
-    rc = upload_csr(g->row, g->adj, g->n, g->pad_row[0], g->pad_deg[0], g->pad_adj[0], &s->dg.d_row, &s->dg.d_deg,
+    rc = upload_csr(g, g->row, g->adj, g->n, g->pad_row[0], g->pad_deg[0], g->pad_adj[0], &s->dg.d_row, &s->dg.d_deg,
                     &s->dg.d_adj, ctx.stream);
     if (rc) return rc;
     s->dg.has_undirected = true;
@@ -995,11 +1066,11 @@ int dm_count_near_cliques(dm_graph* g, int32_t n, const dm_opts* o, uint64_t* co
   const int c = n - 2;
   const int need = c - 1;  // out-neighbours a root needs to start a c-clique
   const int world = (o && o->world_size > 1) ? o->world_size : 1;
-  int n_roots = need <= g->max_out_degree ? (int)s->cnt_ge[need] : 0;
+  int n_roots = need <= g->max_out_degree ? (int)g->cnt_ge[need] : 0;
   const int32_t* d_roots = s->d_deg_order;
   if (world > 1) {
     std::vector<int32_t> mine;
-    for (int i = o->rank; i < n_roots; i += world) mine.push_back(s->deg_order[i]);
+    for (int i = o->rank; i < n_roots; i += world) mine.push_back(g->deg_order[i]);
     if ((rc = ensure_ws_bytes(reinterpret_cast<void**>(&ws.d_tasks), &ws.tasks_cap,
                               sizeof(int32_t) * (mine.size() + 1))))
       return rc;
@@ -1078,7 +1149,7 @@ int dm_count_motifs(dm_graph* g, int32_t k, const dm_dictionary* dict, const dm_
   if ((rc = prepare_ws(ws, ctx.stream))) return rc;
   DM_CUDA(cudaEventRecord(ws.ev0, ctx.stream));
   if (!s->dg.has_undirected) {
-    rc = upload_csr(g->row, g->adj, g->n, g->pad_row[0], g->pad_deg[0], g->pad_adj[0], &s->dg.d_row,
+    rc = upload_csr(g, g->row, g->adj, g->n, g->pad_row[0], g->pad_deg[0], g->pad_adj[0], &s->dg.d_row,
                     &s->dg.d_deg, &s->dg.d_adj, ctx.stream);
     if (rc) return rc;
     s->dg.has_undirected = true;
@@ -1093,15 +1164,17 @@ int dm_count_motifs(dm_graph* g, int32_t k, const dm_dictionary* dict, const dm_
   const int32_t* d_roots = nullptr;
   int n_roots = 0;
   if (!s->d_up_order) {
-    std::vector<int32_t> order;
-    for (int32_t v = 0; v < g->n; ++v)
-      if (upper(v) > 0) order.push_back(v);
-    std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) { return upper(a) > upper(b); });
-    DM_CUDA(cudaMalloc(&s->d_up_order, sizeof(int32_t) * std::max<size_t>(order.size(), 1)));
+    std::vector<int32_t>& order = g->up_order;
+    if (order.empty()) {
+      for (int32_t v = 0; v < g->n; ++v)
+        if (upper(v) > 0) order.push_back(v);
+      std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) { return upper(a) > upper(b); });
+      pin_host(g, order.data(), sizeof(int32_t) * order.size());
+    }
+    DM_CUDA(gbuf_alloc(reinterpret_cast<void**>(&s->d_up_order), sizeof(int32_t) * std::max<size_t>(order.size(), 1)));
     if (!order.empty())
       DM_CUDA(cudaMemcpyAsync(s->d_up_order, order.data(), sizeof(int32_t) * order.size(), cudaMemcpyHostToDevice,
                               ctx.stream));
-    DM_CUDA(cudaStreamSynchronize(ctx.stream));
     s->n_up = (int)order.size();
   }
   std::vector<int32_t> roots, parts;

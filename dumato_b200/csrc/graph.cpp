@@ -616,6 +616,7 @@ int dm_motif_work_model(dm_graph* g, int32_t k, uint64_t* nodes_out, uint64_t* b
 void dm_graph_free(dm_graph* g) {
   if (!g) return;
   release_device_graphs(g);
+  unpin_host_arrays(g);
   delete g;
 }
 
