@@ -12,9 +12,10 @@
 //   bitmap path (out-degree d <= 64*NWMAX, NWMAX <= 4): the warp builds the local
 //       adjacency bitmap of the root's out-neighbourhood L in shared memory (bit j of row i
 //       set iff L[j] in N+(L[i])). Items are the local edges (c1, c2); a lane takes an item
-//       and counts the (k-3)-cliques of row[c1] & row[c2] by its own DFS over 64-bit words:
-//       extend = AND of two rows, compact = nothing (bit order is candidate order),
-//       aggregate = popc at the last level.
+//       and counts the (k-3)-cliques of row[c1] & row[c2] by a depth-first walk over 64-bit
+//       words that the warp's lanes step in lockstep (Walk, lockstep_items): extend = AND of
+//       two rows, compact = nothing (bit order is candidate order), aggregate = popc at the
+//       last level.
 //   list path (larger d, or DM_MODE_LIST): the reference's list structure. Items are the
 //       first-level candidates c1; the warp extends sorted candidate lists level by level in
 //       a per-warp global arena with dm_gpm::extend_intersect (a merge of lane slices, or a
@@ -43,61 +44,22 @@ __device__ __forceinline__ int popc(const Bits<NW>& s) {
   return c;
 }
 
-// Number of (D+1)-cliques inside the local vertex set S (rows: NW u64 words per row).
-template <int D, int NW>
-__device__ __forceinline__ unsigned long long count_rec(const Bits<NW>& S, const uint64_t* __restrict__ rows) {
-  if constexpr (D == 0) {
-    return (unsigned long long)popc(S);
-  } else {
-    unsigned long long sum = 0;
+// Select the j-th set bit of a register bitset.
+template <int NW>
+__device__ __forceinline__ int select_bits(const Bits<NW>& S, int j) {
 #pragma unroll
-    for (int wi = 0; wi < NW; ++wi) {
-      uint64_t bits = S.w[wi];
-      while (bits) {
-        const int b = __ffsll((long long)bits) - 1;
-        bits &= bits - 1;
-        const uint64_t* rc = rows + (wi * 64 + b) * NW;
-        Bits<NW> T;
-#pragma unroll
-        for (int j = 0; j < NW; ++j) T.w[j] = (j < wi ? 0ull : (j == wi ? bits : S.w[j])) & rc[j];
-        if constexpr (D == 1) {
-          sum += (unsigned long long)popc(T);
-        } else {
-          if (popc(T) >= D) sum += count_rec<D - 1, NW>(T, rows);
-        }
-      }
+  for (int w = 0; w < NW; ++w) {
+    const uint64_t x = S.w[w];
+    const int pc = __popcll(x);
+    if (j < pc) {
+      const unsigned lo = (unsigned)x;
+      const int pl = __popc(lo);
+      if (j < pl) return w * 64 + (int)__fns(lo, 0, j + 1);
+      return w * 64 + 32 + (int)__fns((unsigned)(x >> 32), 0, j - pl + 1);
     }
-    return sum;
+    j -= pc;
   }
-}
-
-// count_rec at the top of a long item, reporting progress to the load balancer's watched
-// word every 16 subtrees: waiting warps treat a word that stops changing for the timeout as
-// a lost wake-up, so an item that runs for seconds on one lane must keep it moving.
-template <int D, int NW>
-__device__ __forceinline__ unsigned long long count_rec_hb(const Bits<NW>& S, const uint64_t* __restrict__ rows,
-                                                           unsigned long long* progress) {
-  if constexpr (D < 3) {
-    return count_rec<D, NW>(S, rows);
-  } else {
-    unsigned long long sum = 0;
-    unsigned sub = 0;
-#pragma unroll
-    for (int wi = 0; wi < NW; ++wi) {
-      uint64_t bits = S.w[wi];
-      while (bits) {
-        const int b = __ffsll((long long)bits) - 1;
-        bits &= bits - 1;
-        const uint64_t* rc = rows + (wi * 64 + b) * NW;
-        Bits<NW> T;
-#pragma unroll
-        for (int j = 0; j < NW; ++j) T.w[j] = (j < wi ? 0ull : (j == wi ? bits : S.w[j])) & rc[j];
-        if (popc(T) >= D) sum += count_rec<D - 1, NW>(T, rows);
-        if ((++sub & 15) == 0) atomicAdd(progress, 1ull);
-      }
-    }
-    return sum;
-  }
+  return -1;
 }
 
 // Position of the j-th (0-based) set bit of an NW-word row.
@@ -223,75 +185,223 @@ static __device__ __forceinline__ void build_local_rows(const int32_t* adj, cons
   }
 }
 
+// The per-task words of a warp (shared memory).
+struct TaskWords {
+  unsigned long long* range;  // item (or position) range: next | end << 32
+  int* don;                   // donations left to the task
+  int* busy;                  // serialises donations
+  int* hn;                    // deferred heavy items
+  int* heavy;                 // their item indices
+};
+
+// Per-lane clique counts by size (the fused count of every k up to K): c[s] = s-cliques.
+template <int K>
+struct Acc {
+  unsigned long long c[K + 1];
+};
+
+// ---------------- lockstep walk ----------------
+//
+// A lane's share of a task is a depth-first walk over candidate sets, kept as an explicit
+// stack of bitsets in registers, and each iteration of the warp's loop expands exactly one
+// node on every lane that has one: pop the lowest member x of the top set and form
+// T = (the rest of that set) & row[x]. All lanes run the same instructions on their own sets,
+// so a warp costs about the largest lane's node count, where nested per-lane recursion costs,
+// level by level, the sum of subtrees that the lanes reach at different loop positions. Lanes
+// whose walk has ended take new items together, with one shared-memory atomic for all of
+// them.
+//
+// Stack entry j holds the candidates for clique vertex LEV0 + j (vertices numbered from 1,
+// the root first). Fused counts (MULTI): a set X formed for entry j adds |X| to c[LEV0 + j]
+// and is expanded while LEV0 + j < K and |X| >= 2. One size K: |X| counts only at entry
+// K - LEV0, and a set is kept only while it can still complete a K-clique. `live` has bit j
+// set while entry j holds members.
+constexpr int REFILL_MIN = 8;    // idle lanes that take new items while other lanes still walk
+constexpr int CHECK_EVERY = 64;  // loop iterations between two donation checks (lane 0)
+
+template <int K, int NW, bool MULTI, int LEV0>
+struct Walk {
+  static constexpr int D = K - LEV0 > 0 ? K - LEV0 : 1;
+  Bits<NW> st[D];
+  int top = -1;
+  unsigned live = 0u;
+
+  // S: the candidates for vertex LEV0.
+  __device__ __forceinline__ void start(const Bits<NW>& S, Acc<K>& acc, unsigned long long& cnt) {
+    const int p = popc(S);
+    if constexpr (MULTI) {
+      acc.c[LEV0] += (unsigned long long)p;
+      if constexpr (LEV0 < K) {
+        if (p >= 2) {
+          st[0] = S;
+          top = 0;
+          live = 1u;
+        }
+      }
+    } else {
+      if constexpr (LEV0 == K) {
+        cnt += (unsigned long long)p;
+      } else if (p >= K - LEV0 + 1) {
+        st[0] = S;
+        top = 0;
+        live = 1u;
+      }
+    }
+  }
+
+  // Expands one node of this lane's walk (top >= 0).
+  __device__ __forceinline__ void step(const uint64_t* __restrict__ rows, Acc<K>& acc, unsigned long long& cnt) {
+    if constexpr (LEV0 < K) {
+      const int j = top;
+      Bits<NW> cur;
+#pragma unroll
+      for (int q = 0; q < D; ++q)
+        if (q == j) cur = st[q];
+      int x = 0;
+      bool found = false;
+#pragma unroll
+      for (int w = 0; w < NW; ++w) {
+        if (!found && cur.w[w] != 0ull) {
+          x = w * 64 + __ffsll((long long)cur.w[w]) - 1;
+          cur.w[w] &= cur.w[w] - 1ull;
+          found = true;
+        }
+      }
+      const uint64_t* rx = rows + x * NW;
+      Bits<NW> T;
+#pragma unroll
+      for (int w = 0; w < NW; ++w) T.w[w] = cur.w[w] & rx[w];
+      const int pc = popc(T);
+      bool push = false;
+      if constexpr (MULTI) {
+#pragma unroll
+        for (int q = 0; q < D; ++q)
+          if (q == j) acc.c[LEV0 + q + 1] += (unsigned long long)pc;
+        push = LEV0 + j + 1 < K && pc >= 2;
+      } else {
+        if (LEV0 + j + 1 == K) cnt += (unsigned long long)pc;
+        else push = pc >= K - LEV0 - j;
+        // members left at this entry need K - LEV0 - j more vertices above them
+        if (popc(cur) <= K - LEV0 - j) {
+#pragma unroll
+          for (int w = 0; w < NW; ++w) cur.w[w] = 0ull;
+        }
+      }
+      uint64_t any = 0ull;
+#pragma unroll
+      for (int w = 0; w < NW; ++w) any |= cur.w[w];
+#pragma unroll
+      for (int q = 0; q < D; ++q)
+        if (q == j) st[q] = cur;
+      if (!any) live &= ~(1u << j);
+      if (push) {
+#pragma unroll
+        for (int q = 1; q < D; ++q)
+          if (q == j + 1) st[q] = T;
+        live |= 1u << (j + 1);
+        top = j + 1;
+      } else if (!any) {
+        top = live ? 31 - __clz((int)live) : -1;
+      }
+    }
+  }
+};
+
+// Warp-lifetime state of the donation checks (lane 0): the hungry/queued counters loaded at
+// the previous check, still in flight until the next one uses them, and the loop iterations
+// run so far, across tasks.
+struct CheckState {
+  int hungry = 0;
+  int queued = 0;
+  unsigned iter = 0u;
+};
+
+__device__ __forceinline__ unsigned lanemask_lt() {
+  unsigned m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+// The warp's loop over the items of tw.range: idle lanes take items (start_item(i) gives a
+// lane item i), walking lanes expand one node each. Lane 0 decides on donations from the
+// counters it sampled at its previous check (the loads stay in flight meanwhile): after every
+// refill that leaves items in the range, and every CHECK_EVERY iterations, where it also
+// takes a new sample; range_maybe_donate then splits the range. Items split off that no
+// queue slot took are run after the range. Returns when every item is done.
+template <int K, int NW, bool MULTI, int LEV0, class StartFn>
+__device__ __forceinline__ void lockstep_items(const LBArgs& lb, const TaskWords& tw, Walk<K, NW, MULTI, LEV0>& wk,
+                                               StartFn&& start_item, const uint64_t* rows, Acc<K>& acc,
+                                               unsigned long long& cnt, int root, long long t_start, int cost_tail,
+                                               int min_items, int level, const int* path, bool eager,
+                                               CheckState& cs) {
+  const int lane = lane_id();
+  bool open = true;
+  int xb = 0, xe = 0;  // lane 0: split-off items to run after the range
+  // lane 0: split the range if the sampled demand asks for it
+  auto maybe_donate = [&]() {
+    if (lb.hungry_trigger > 0 && xe <= xb && (cs.hungry - cs.queued >= lb.hungry_trigger || eager)) {
+      int ob = 0, oe = 0;
+      if (range_maybe_donate(lb, tw.range, root, tw.don, t_start, tw.busy, ob, oe, cost_tail, min_items, level, path,
+                             eager)) {
+        xb = ob;
+        xe = oe;
+      }
+    }
+  };
+  while (true) {
+    const unsigned idle = __ballot_sync(FULL_MASK, wk.top < 0);
+    if (open && idle != 0u && (idle == FULL_MASK || __popc(idle) >= REFILL_MIN)) {
+      const int leader = __ffs(idle) - 1;
+      const int want = __popc(idle);
+      unsigned long long old = 0ull;
+      if (lane == leader) old = atomicAdd(tw.range, (unsigned long long)want);
+      old = __shfl_sync(FULL_MASK, old, leader);
+      const int next = (int)(unsigned)old, end = (int)(unsigned)(old >> 32);
+      if (wk.top < 0) {
+        const int my = next + __popc(idle & lanemask_lt());
+        if (my < end) start_item(my);
+      }
+      if (next + want < end) {
+        if (lane == 0) maybe_donate();
+        __syncwarp();
+      } else {
+        const int has = __shfl_sync(FULL_MASK, xe > xb ? 1 : 0, 0);
+        if (has) {
+          const int b0 = __shfl_sync(FULL_MASK, xb, 0), e0 = __shfl_sync(FULL_MASK, xe, 0);
+          if (lane == 0) {
+            *tw.range = pack_range(b0, e0);
+            xb = xe = 0;
+          }
+          __syncwarp();
+        } else {
+          open = false;
+        }
+      }
+    }
+    const unsigned walking = __ballot_sync(FULL_MASK, wk.top >= 0);
+    if (walking == 0u) {
+      if (!open) break;
+      continue;
+    }
+    if (wk.top >= 0) wk.step(rows, acc, cnt);
+    if (++cs.iter % CHECK_EVERY == 0u) {
+      if (lane == 0) {
+        atomicAdd(&lb.ctr->progress, (unsigned long long)CHECK_EVERY);
+        if (lb.hungry_trigger > 0) {
+          if (open) maybe_donate();
+          // read at the next check: the warp walks on while the loads complete
+          cs.hungry = vload(&lb.ctr->hungry);
+          cs.queued = vload(&lb.ctr->queued);
+        }
+      }
+      __syncwarp();
+    }
+  }
+}
+
 constexpr int HEAVY_BITS = 24;  // an item whose candidate set has this many members is
                                 // run by the whole warp instead of one lane (k >= 6)
 constexpr int HEAVY_SLOTS = 32;
-
-// Counts the cliques of item `it` (a local edge c1 < c2, or a row c1 when k == 3) on one
-// lane. For k >= 6 an item with a large candidate set is deferred to the warp instead
-// (returns without counting) when a heavy slot is free.
-template <int K, int NW>
-__device__ __forceinline__ unsigned long long bitmap_item(int it, const uint64_t* rows, const int32_t* sE, int d,
-                                                          int* hn, int* heavy, unsigned long long* progress) {
-  if constexpr (K == 3) {
-    Bits<NW> S;
-#pragma unroll
-    for (int w = 0; w < NW; ++w) S.w[w] = rows[it * NW + w];
-    return (unsigned long long)popc(S);
-  } else {
-    const int c1 = lower_bound(sE, 0, d + 1, it + 1) - 1;
-    const int c2 = select_bit<NW>(rows + c1 * NW, it - sE[c1]);
-    Bits<NW> S;
-#pragma unroll
-    for (int w = 0; w < NW; ++w) S.w[w] = rows[c1 * NW + w] & rows[c2 * NW + w];
-    if constexpr (K == 4) {
-      return (unsigned long long)popc(S);
-    } else {
-      const int p = popc(S);
-      if (p < K - 3) return 0;
-      if constexpr (K >= 6) {
-        if (p >= HEAVY_BITS && hn) {
-          const int slot = atomicAdd(hn, 1);
-          if (slot < HEAVY_SLOTS) {
-            heavy[slot] = it;
-            return 0;
-          }
-        }
-      }
-      return count_rec_hb<(K >= 5 ? K - 4 : 0), NW>(S, rows, progress);
-    }
-  }
-}
-
-// Warp-cooperative run of one heavy item: the third local vertex c3 is spread over the
-// lanes (the j-th member of the candidate set goes to lane j mod 32).
-template <int K, int NW>
-__device__ __forceinline__ unsigned long long heavy_item(int it, const uint64_t* rows, const int32_t* sE, int d,
-                                                         unsigned long long* progress) {
-  const int lane = lane_id();
-  const int c1 = lower_bound(sE, 0, d + 1, it + 1) - 1;
-  const int c2 = select_bit<NW>(rows + c1 * NW, it - sE[c1]);
-  Bits<NW> S;
-#pragma unroll
-  for (int w = 0; w < NW; ++w) S.w[w] = rows[c1 * NW + w] & rows[c2 * NW + w];
-  unsigned long long sum = 0;
-  int j = 0;
-#pragma unroll
-  for (int wi = 0; wi < NW; ++wi) {
-    uint64_t bits = S.w[wi];
-    while (bits) {
-      const int b = __ffsll((long long)bits) - 1;
-      bits &= bits - 1;
-      if ((j++ & 31) != lane) continue;
-      const uint64_t* rc = rows + (wi * 64 + b) * NW;
-      Bits<NW> T;
-#pragma unroll
-      for (int w = 0; w < NW; ++w) T.w[w] = (w < wi ? 0ull : (w == wi ? bits : S.w[w])) & rc[w];
-      if (popc(T) >= K - 4) sum += count_rec_hb<(K >= 6 ? K - 5 : 0), NW>(T, rows, progress);
-    }
-  }
-  return sum;
-}
 
 // Bitmap path for one task. Returns the k-cliques counted by this lane.
 template <int K, int NW, int M>
@@ -309,6 +419,12 @@ __device__ unsigned long long bitmap_task(const CliqueArgs& a, unsigned char* ws
   int* hn = reinterpret_cast<int*>(wsm + LY.hn);
   int* heavy = reinterpret_cast<int*>(wsm + LY.heavy);
   const long long t_start = global_ns();
+  // the donation checks' first sample is loaded while the bitmaps are built
+  CheckState cs;
+  if (lane == 0 && a.lb.hungry_trigger > 0) {
+    cs.hungry = vload(&a.lb.ctr->hungry);
+    cs.queued = vload(&a.lb.ctr->queued);
+  }
   for (int i = lane; i < d * RW; i += 32) rows32[i] = 0;
   // sE holds the members' row starts while the rows are built, the item prefix after
   const int total = load_root_list(a.g, root, d, sL, sP, sE);
@@ -350,29 +466,87 @@ __device__ unsigned long long bitmap_task(const CliqueArgs& a, unsigned char* ws
   }
   __syncwarp();
   unsigned long long cnt = 0;
-  unsigned done = 0;
-  while (true) {
-    const int it = range_take(range);
-    if (it < 0) break;
-    cnt += bitmap_item<K, NW>(it, rows, sE, d, hn, heavy, &a.lb.ctr->progress);
-    if ((++done & 15) == 0) {
-      int ob = 0, oe = 0;
-      if (range_maybe_donate(a.lb, range, root, donations_left, t_start, busy, ob, oe)) {
-        for (int j = ob; j < oe; ++j) cnt += bitmap_item<K, NW>(j, rows, sE, d, nullptr, nullptr, &a.lb.ctr->progress);
+  if constexpr (K == 3) {
+    // items are the rows: one popcount each, the lanes stay together
+    unsigned done = 0;
+    while (true) {
+      const int it = range_take(range);
+      if (it < 0) break;
+      Bits<NW> S;
+#pragma unroll
+      for (int w = 0; w < NW; ++w) S.w[w] = rows[it * NW + w];
+      cnt += (unsigned long long)popc(S);
+      if ((++done & 15) == 0) {
+        int ob = 0, oe = 0;
+        if (range_maybe_donate(a.lb, range, root, donations_left, t_start, busy, ob, oe)) {
+          for (int j = ob; j < oe; ++j) {
+            Bits<NW> U;
+#pragma unroll
+            for (int w = 0; w < NW; ++w) U.w[w] = rows[j * NW + w];
+            cnt += (unsigned long long)popc(U);
+          }
+        }
       }
-      if ((done & 255) == 0) atomicAdd(&a.lb.ctr->progress, 256ull);
-    }
-  }
-  __syncwarp();
-  if constexpr (K >= 6) {
-    const int nh = min(*hn, HEAVY_SLOTS);
-    for (int h = 0; h < nh; ++h) {
-      cnt += heavy_item<K, NW>(heavy[h], rows, sE, d, &a.lb.ctr->progress);
-      if (lane == 0) atomicAdd(&a.lb.ctr->progress, 1ull);
     }
     __syncwarp();
+    return cnt;
+  } else {
+    const TaskWords tw{range, donations_left, busy, hn, heavy};
+    Acc<K> unused;
+    Walk<K, NW, false, 4> wk;
+    auto start_item = [&](int i) {
+      const int c1 = lower_bound(sE, 0, d + 1, i + 1) - 1;
+      const int c2 = select_bit<NW>(rows + c1 * NW, i - sE[c1]);
+      Bits<NW> S;
+#pragma unroll
+      for (int w = 0; w < NW; ++w) S.w[w] = rows[c1 * NW + w] & rows[c2 * NW + w];
+      if constexpr (K >= 6) {
+        // a large candidate set is run by the whole warp after the range
+        if (popc(S) >= HEAVY_BITS) {
+          const int slot = atomicAdd(hn, 1);
+          if (slot < HEAVY_SLOTS) {
+            heavy[slot] = i;
+            return;
+          }
+        }
+      }
+      wk.start(S, unused, cnt);
+    };
+    lockstep_items<K, NW, false, 4>(a.lb, tw, wk, start_item, rows, unused, cnt, root, t_start, 0, 0, 0, nullptr, false,
+                                    cs);
+    __syncwarp();
+    if constexpr (K >= 6) {
+      // heavy items: the members of S (clique vertex 4) are spread over the lanes; this
+      // kernel takes no level-1 donations, so these ranges are never split
+      const int nh = min(*hn, HEAVY_SLOTS);
+      for (int h = 0; h < nh; ++h) {
+        const int it = heavy[h];
+        const int c1 = lower_bound(sE, 0, d + 1, it + 1) - 1;
+        const int c2 = select_bit<NW>(rows + c1 * NW, it - sE[c1]);
+        Bits<NW> S;
+#pragma unroll
+        for (int w = 0; w < NW; ++w) S.w[w] = rows[c1 * NW + w] & rows[c2 * NW + w];
+        __syncwarp();
+        if (lane == 0) *range = pack_range(0, popc(S));
+        __syncwarp();
+        Walk<K, NW, false, 5> hw;
+        auto start_pos = [&](int j) {
+          const int c3 = select_bits<NW>(S, j);
+          const int w3 = c3 >> 6;
+          const uint64_t above = (c3 & 63) == 63 ? 0ull : (~0ull << ((c3 & 63) + 1));
+          const uint64_t* rc = rows + c3 * NW;
+          Bits<NW> T;
+#pragma unroll
+          for (int w = 0; w < NW; ++w) T.w[w] = (w < w3 ? 0ull : (w == w3 ? (S.w[w] & above) : S.w[w])) & rc[w];
+          hw.start(T, unused, cnt);
+        };
+        lockstep_items<K, NW, false, 5>(a.lb, tw, hw, start_pos, rows, unused, cnt, root, t_start, 0, INT_MAX, 0,
+                                        nullptr, false, cs);
+        __syncwarp();
+      }
+    }
+    return cnt;
   }
-  return cnt;
 }
 
 // List path for one task. The warp's lanes form groups of W (the reference's virtual warps,

@@ -184,24 +184,6 @@ struct CachedArgs {
                                // at n_static
 };
 
-// Select the j-th set bit of a register bitset.
-template <int NW>
-__device__ __forceinline__ int select_bits(const Bits<NW>& S, int j) {
-#pragma unroll
-  for (int w = 0; w < NW; ++w) {
-    const uint64_t x = S.w[w];
-    const int pc = __popcll(x);
-    if (j < pc) {
-      const unsigned lo = (unsigned)x;
-      const int pl = __popc(lo);
-      if (j < pl) return w * 64 + (int)__fns(lo, 0, j + 1);
-      return w * 64 + 32 + (int)__fns((unsigned)(x >> 32), 0, j - pl + 1);
-    }
-    j -= pc;
-  }
-  return -1;
-}
-
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
@@ -241,114 +223,15 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* mbar, unsigned parity) {
   return false;
 }
 
-// The per-task words of a warp (shared memory).
-struct TaskWords {
-  unsigned long long* range;  // item (or position) range: next | end << 32
-  int* don;                   // donations left to the task
-  int* busy;                  // serialises donations
-  int* hn;                    // deferred heavy items
-  int* heavy;                 // their item indices
-};
-
-// Per-lane clique counts by size (the fused count of every k up to K): c[s] = s-cliques.
-template <int K>
-struct Acc {
-  unsigned long long c[K + 1];
-};
-
-// Fused counting below a candidate set S whose members would be the S0-th vertex of a clique:
-// c[S0] += |S|, and for every x in S the cliques of S_{>x} & N(x) count at S0 + 1, down to
-// c[S0 + L]. Unlike count_rec no subtree is pruned for being too small to reach K, since its
-// smaller cliques count too.
-template <int L, int NW, int K, int S0>
-__device__ __forceinline__ void count_all(const Bits<NW>& S, const uint64_t* __restrict__ rows, Acc<K>& acc) {
-  acc.c[S0] += (unsigned long long)popc(S);
-  if constexpr (L > 0) {
-#pragma unroll
-    for (int wi = 0; wi < NW; ++wi) {
-      uint64_t bits = S.w[wi];
-      while (bits) {
-        const int b = __ffsll((long long)bits) - 1;
-        bits &= bits - 1;
-        const uint64_t* rc = rows + (wi * 64 + b) * NW;
-        Bits<NW> T;
-        uint64_t any = 0;
-#pragma unroll
-        for (int j = 0; j < NW; ++j) {
-          T.w[j] = (j < wi ? 0ull : (j == wi ? bits : S.w[j])) & rc[j];
-          any |= T.w[j];
-        }
-        if (any) count_all<L - 1, NW, K, S0 + 1>(T, rows, acc);
-      }
-    }
-  }
-}
-
-// count_all at the top of a long item, moving the load balancer's watched word every 16
-// subtrees (see count_rec_hb).
-template <int L, int NW, int K, int S0>
-__device__ __forceinline__ void count_all_hb(const Bits<NW>& S, const uint64_t* __restrict__ rows, Acc<K>& acc,
-                                             unsigned long long* progress) {
-  if constexpr (L < 3) {
-    count_all<L, NW, K, S0>(S, rows, acc);
-  } else {
-    acc.c[S0] += (unsigned long long)popc(S);
-    unsigned sub = 0;
-#pragma unroll
-    for (int wi = 0; wi < NW; ++wi) {
-      uint64_t bits = S.w[wi];
-      while (bits) {
-        const int b = __ffsll((long long)bits) - 1;
-        bits &= bits - 1;
-        const uint64_t* rc = rows + (wi * 64 + b) * NW;
-        Bits<NW> T;
-        uint64_t any = 0;
-#pragma unroll
-        for (int j = 0; j < NW; ++j) {
-          T.w[j] = (j < wi ? 0ull : (j == wi ? bits : S.w[j])) & rc[j];
-          any |= T.w[j];
-        }
-        if (any) count_all<L - 1, NW, K, S0 + 1>(T, rows, acc);
-        if ((++sub & 15) == 0) atomicAdd(progress, 1ull);
-      }
-    }
-  }
-}
-
-// Fused counting of item `it` (the local edge c1 < c2 of the root): the item is a triangle,
-// its candidate set S = row[c1] & row[c2] holds the 4-cliques, and so on down to K. For
-// K >= 6 an item with a large S is deferred to the warp after its 4-cliques are counted.
-template <int K, int NW>
-__device__ __forceinline__ void bitmap_item_all(int it, const uint64_t* rows, const int32_t* sE, int d, int* hn,
-                                                int* heavy, unsigned long long* progress, Acc<K>& acc) {
-  acc.c[3] += 1ull;
-  const int c1 = lower_bound(sE, 0, d + 1, it + 1) - 1;
-  const int c2 = select_bit<NW>(rows + c1 * NW, it - sE[c1]);
-  Bits<NW> S;
-#pragma unroll
-  for (int w = 0; w < NW; ++w) S.w[w] = rows[c1 * NW + w] & rows[c2 * NW + w];
-  if constexpr (K >= 6) {
-    const int p = popc(S);
-    if (p >= HEAVY_BITS && hn) {
-      const int slot = atomicAdd(hn, 1);
-      if (slot < HEAVY_SLOTS) {
-        heavy[slot] = it;
-        acc.c[4] += (unsigned long long)p;
-        return;
-      }
-    }
-  }
-  count_all_hb<K - 4, NW, K, 4>(S, rows, acc, progress);
-}
-
 // Level-1 task: positions [lo, hi) (hi < 0: to the end) of the candidate set S of item
-// `it` choose the third local vertex c3; each lane counts the (k-3)-cliques of
-// S_{>c3} & row[c3] for the positions it takes. While warps are hungry the upper half of
-// the positions left is donated as (root, level 1, path = {it}, range).
+// `it` (the root, c1 and c2 are clique vertices 1..3) choose vertex 4, c3; each lane walks
+// S_{>c3} & row[c3], the candidates for vertex 5, for the positions it takes. While warps
+// are hungry the upper part of the positions left is donated as (root, level 1, path = {it},
+// range).
 template <int K, int NW, bool MULTI>
-__device__ unsigned long long heavy_run(const CachedArgs& a, const TaskWords& tw, const uint64_t* rows,
-                                        const int32_t* sE, int d, int root, int it, int lo, int hi, bool eager,
-                                        Acc<K>& acc) {
+__device__ __forceinline__ unsigned long long heavy_run(const CachedArgs& a, const TaskWords& tw, const uint64_t* rows,
+                                                        const int32_t* sE, int d, int root, int it, int lo, int hi,
+                                                        bool eager, Acc<K>& acc, CheckState& cs) {
   const int lane = lane_id();
   const int c1 = lower_bound(sE, 0, d + 1, it + 1) - 1;
   const int c2 = select_bit<NW>(rows + c1 * NW, it - sE[c1]);
@@ -364,11 +247,11 @@ __device__ unsigned long long heavy_run(const CachedArgs& a, const TaskWords& tw
     *tw.busy = 0;
   }
   __syncwarp();
-  const long long t_start = global_ns();
+  const long long t_start = lane == 0 ? global_ns() : 0;
   const int path[1] = {it};
   unsigned long long cnt = 0;
-  int j;
-  while ((j = range_take(tw.range)) >= 0) {
+  Walk<K, NW, MULTI, 5> wk;
+  auto start_pos = [&](int j) {
     const int c3 = select_bits<NW>(S, j);
     const int w3 = c3 >> 6;
     const uint64_t above = (c3 & 63) == 63 ? 0ull : (~0ull << ((c3 & 63) + 1));
@@ -376,25 +259,9 @@ __device__ unsigned long long heavy_run(const CachedArgs& a, const TaskWords& tw
     Bits<NW> T;
 #pragma unroll
     for (int w = 0; w < NW; ++w) T.w[w] = (w < w3 ? 0ull : (w == w3 ? (S.w[w] & above) : S.w[w])) & rc[w];
-    if constexpr (MULTI) count_all_hb<K - 5, NW, K, 5>(T, rows, acc, &a.c.lb.ctr->progress);
-    else if (popc(T) >= K - 4) cnt += count_rec_hb<(K >= 6 ? K - 5 : 0), NW>(T, rows, &a.c.lb.ctr->progress);
-    // every position is a whole subtree below level 2: check for hungry warps after each
-    {
-      int ob = 0, oe = 0;
-      if (range_maybe_donate(a.c.lb, tw.range, root, tw.don, t_start, tw.busy, ob, oe, p, 2, 1, path, eager)) {
-        for (int q = ob; q < oe; ++q) {
-          const int c = select_bits<NW>(S, q);
-          const int wq = c >> 6;
-          const uint64_t ab = (c & 63) == 63 ? 0ull : (~0ull << ((c & 63) + 1));
-          Bits<NW> U;
-#pragma unroll
-          for (int w = 0; w < NW; ++w) U.w[w] = (w < wq ? 0ull : (w == wq ? (S.w[w] & ab) : S.w[w])) & rows[c * NW + w];
-          if constexpr (MULTI) count_all_hb<K - 5, NW, K, 5>(U, rows, acc, &a.c.lb.ctr->progress);
-          else if (popc(U) >= K - 4) cnt += count_rec_hb<(K >= 6 ? K - 5 : 0), NW>(U, rows, &a.c.lb.ctr->progress);
-        }
-      }
-    }
-  }
+    wk.start(T, acc, cnt);
+  };
+  lockstep_items<K, NW, MULTI, 5>(a.c.lb, tw, wk, start_pos, rows, acc, cnt, root, t_start, p, 2, 1, path, eager, cs);
   __syncwarp();
   return cnt;
 }
@@ -403,9 +270,10 @@ __device__ unsigned long long heavy_run(const CachedArgs& a, const TaskWords& tw
 // encoding; items are the local edges, or the rows when k == 3), level 1 runs positions
 // [b, e) of item `it`'s candidate set. Returns this lane's share.
 template <int K, int NW, bool MULTI>
-__device__ unsigned long long staged_run(const CachedArgs& a, const TaskWords& tw, const uint64_t* rows,
-                                         int32_t* sE, int root, int d, int b, int e, int level, int it, bool eager,
-                                         Acc<K>& acc) {
+__device__ __forceinline__ unsigned long long staged_run(const CachedArgs& a, const TaskWords& tw,
+                                                         const uint64_t* rows, int32_t* sE, int root, int d, int b,
+                                                         int e, int level, int it, bool eager, Acc<K>& acc,
+                                                         CheckState& cs) {
   const int lane = lane_id();
   int n_items;
   if constexpr (K >= 4) {
@@ -433,7 +301,7 @@ __device__ unsigned long long staged_run(const CachedArgs& a, const TaskWords& t
   }
   __syncwarp();
   if constexpr (K >= 6) {
-    if (level == 1) return heavy_run<K, NW, MULTI>(a, tw, rows, sE, d, root, it, b, e, eager, acc);
+    if (level == 1) return heavy_run<K, NW, MULTI>(a, tw, rows, sE, d, root, it, b, e, eager, acc, cs);
   }
   int lo, hi;
   task_range(b, e, n_items, lo, hi);
@@ -444,48 +312,81 @@ __device__ unsigned long long staged_run(const CachedArgs& a, const TaskWords& t
     *tw.hn = 0;
   }
   __syncwarp();
-  const long long t_start = global_ns();
+  const long long t_start = lane == 0 ? global_ns() : 0;
   unsigned long long cnt = 0;
-  unsigned done = 0;
-  int x;
-  while ((x = range_take(tw.range)) >= 0) {
-    if constexpr (MULTI) bitmap_item_all<K, NW>(x, rows, sE, d, tw.hn, tw.heavy, &a.c.lb.ctr->progress, acc);
-    else cnt += bitmap_item<K, NW>(x, rows, sE, d, tw.hn, tw.heavy, &a.c.lb.ctr->progress);
-    if ((++done & 15) == 0) {
-      int ob = 0, oe = 0;
-      if (range_maybe_donate(a.c.lb, tw.range, root, tw.don, t_start, tw.busy, ob, oe, 0, 0, 0, nullptr, eager)) {
-        for (int j = ob; j < oe; ++j) {
-          if constexpr (MULTI) bitmap_item_all<K, NW>(j, rows, sE, d, nullptr, nullptr, &a.c.lb.ctr->progress, acc);
-          else cnt += bitmap_item<K, NW>(j, rows, sE, d, nullptr, nullptr, &a.c.lb.ctr->progress);
+  if constexpr (K == 3) {
+    // items are the rows: one popcount each, the lanes stay together
+    unsigned done = 0;
+    int x;
+    while ((x = range_take(tw.range)) >= 0) {
+      Bits<NW> S;
+#pragma unroll
+      for (int w = 0; w < NW; ++w) S.w[w] = rows[x * NW + w];
+      cnt += (unsigned long long)popc(S);
+      if ((++done & 15) == 0) {
+        int ob = 0, oe = 0;
+        if (range_maybe_donate(a.c.lb, tw.range, root, tw.don, t_start, tw.busy, ob, oe, 0, 0, 0, nullptr, eager)) {
+          for (int j = ob; j < oe; ++j) {
+            Bits<NW> U;
+#pragma unroll
+            for (int w = 0; w < NW; ++w) U.w[w] = rows[j * NW + w];
+            cnt += (unsigned long long)popc(U);
+          }
         }
       }
-      if ((done & 255) == 0) atomicAdd(&a.c.lb.ctr->progress, 256ull);
     }
-  }
-  __syncwarp();
-  if constexpr (K >= 6) {
-    const int nh = min(*tw.hn, HEAVY_SLOTS);
-    for (int h = 0; h < nh; ++h) {
-      const int hit = tw.heavy[h];
-      cnt += heavy_run<K, NW, MULTI>(a, tw, rows, sE, d, root, hit, 0, -1, eager, acc);
+    __syncwarp();
+    return cnt;
+  } else {
+    Walk<K, NW, MULTI, 4> wk;
+    auto start_item = [&](int i) {
+      if constexpr (MULTI) acc.c[3] += 1ull;
+      const int c1 = lower_bound(sE, 0, d + 1, i + 1) - 1;
+      const int c2 = select_bit<NW>(rows + c1 * NW, i - sE[c1]);
+      Bits<NW> S;
+#pragma unroll
+      for (int w = 0; w < NW; ++w) S.w[w] = rows[c1 * NW + w] & rows[c2 * NW + w];
+      if constexpr (K >= 6) {
+        // a large candidate set is run by the whole warp after the range (heavy_run)
+        const int p = popc(S);
+        if (p >= HEAVY_BITS) {
+          const int slot = atomicAdd(tw.hn, 1);
+          if (slot < HEAVY_SLOTS) {
+            tw.heavy[slot] = i;
+            if constexpr (MULTI) acc.c[4] += (unsigned long long)p;
+            return;
+          }
+        }
+      }
+      wk.start(S, acc, cnt);
+    };
+    lockstep_items<K, NW, MULTI, 4>(a.c.lb, tw, wk, start_item, rows, acc, cnt, root, t_start, 0, 0, 0, nullptr, eager,
+                                    cs);
+    __syncwarp();
+    if constexpr (K >= 6) {
+      const int nh = min(*tw.hn, HEAVY_SLOTS);
+      for (int h = 0; h < nh; ++h) {
+        const int hit = tw.heavy[h];
+        cnt += heavy_run<K, NW, MULTI>(a, tw, rows, sE, d, root, hit, 0, -1, eager, acc, cs);
+      }
     }
+    return cnt;
   }
-  return cnt;
 }
 
 template <int K, int M, bool MULTI>
 __device__ __forceinline__ unsigned long long staged_dispatch(const CachedArgs& a, const TaskWords& tw,
                                                               const uint64_t* rows, int32_t* sE, int root, int d,
                                                               int b, int e, int level, int it, bool eager,
-                                                              Acc<K>& acc) {
+                                                              Acc<K>& acc, CheckState& cs) {
   const int nw = (d + 63) >> 6;
-  if (nw <= 1) return staged_run<K, 1, MULTI>(a, tw, rows, sE, root, d, b, e, level, it, eager, acc);
+  if (nw <= 1) return staged_run<K, 1, MULTI>(a, tw, rows, sE, root, d, b, e, level, it, eager, acc, cs);
   if constexpr (M >= 2)
-    if (nw == 2) return staged_run<K, 2, MULTI>(a, tw, rows, sE, root, d, b, e, level, it, eager, acc);
+    if (nw == 2) return staged_run<K, 2, MULTI>(a, tw, rows, sE, root, d, b, e, level, it, eager, acc, cs);
   if constexpr (M >= 3)
-    if (nw == 3) return staged_run<K, 3, MULTI>(a, tw, rows, sE, root, d, b, e, level, it, eager, acc);
+    if (nw == 3) return staged_run<K, 3, MULTI>(a, tw, rows, sE, root, d, b, e, level, it, eager, acc, cs);
   if constexpr (M >= 4)
-    if (nw == 4) return staged_run<K, 4, MULTI>(a, tw, rows, sE, root, d, b, e, level, it, eager, acc);
+    if (nw == 4) return staged_run<K, 4, MULTI>(a, tw, rows, sE, root, d, b, e, level, it, eager, acc, cs);
   if (lane_id() == 0) set_err(a.c.lb.ctr, ERR_BAD_TASK);
   return 0;
 }
@@ -544,8 +445,13 @@ __device__ __forceinline__ bool stage_blocks(const uint4* blocks, uint4* stage, 
   }
 }
 
+// Blocks per SM the register budget is sized for: the index kernel of rows up to 64 bits
+// keeps four blocks (the shared-memory limit), wider rows two.
+template <int M>
+constexpr int cached_min_blocks() { return M == 1 ? 2 : 2; }
+
 template <int K, int M, bool TMA, bool MULTI>
-__global__ void __launch_bounds__(256) clique_cached_kernel(const __grid_constant__ CachedArgs a) {
+__global__ void __launch_bounds__(256, cached_min_blocks<M>()) clique_cached_kernel(const __grid_constant__ CachedArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
   constexpr CachedWarp LY = cached_layout(M);
   constexpr uint32_t STAGE_UNITS = stage_words(M) / 2;
@@ -579,6 +485,7 @@ __global__ void __launch_bounds__(256) clique_cached_kernel(const __grid_constan
   }
   __syncthreads();
   unsigned long long idle[2] = {0ull, 0ull};
+  CheckState cs;
   Acc<K> acc;
 #pragma unroll
   for (int j = 0; j <= K; ++j) acc.c[j] = 0ull;
@@ -674,7 +581,7 @@ __global__ void __launch_bounds__(256) clique_cached_kernel(const __grid_constan
         } else if (K == 2) {
           if (lane == 0) tc = (unsigned long long)di;
         } else if (ui > 0) {
-          tc = staged_dispatch<K, M, MULTI>(a, tw, srows + 2 * si, sE, r, di, bb, ee, level, it1, eager, acc);
+          tc = staged_dispatch<K, M, MULTI>(a, tw, srows + 2 * si, sE, r, di, bb, ee, level, it1, eager, acc, cs);
         } else if (MULTI && di > a.c.list_threshold) {
           if (lane == 0) set_err(a.c.lb.ctr, ERR_BAD_TASK);  // the fused count runs on the index only
         } else if (di > a.c.list_threshold) {
