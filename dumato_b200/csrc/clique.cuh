@@ -62,6 +62,63 @@ __device__ __forceinline__ int select_bits(const Bits<NW>& S, int j) {
   return -1;
 }
 
+// Position of the k-th (0-based) set bit of a 64-bit word, without branches (a popcount
+// halving search: the lanes of a warp stay together whatever their words).
+__device__ __forceinline__ int select64(uint64_t v, int k) {
+  const unsigned lo = (unsigned)v;
+  const int c = __popc(lo);
+  const bool up = k >= c;
+  k -= up ? c : 0;
+  unsigned w = up ? (unsigned)(v >> 32) : lo;
+  int pos = up ? 32 : 0;
+#pragma unroll
+  for (int s = 16; s >= 1; s >>= 1) {
+    const int cc = __popc(w & ((1u << s) - 1u));
+    const bool u = k >= cc;
+    k -= u ? cc : 0;
+    w = u ? (w >> s) : w;
+    pos += u ? s : 0;
+  }
+  return pos;
+}
+
+// First index i in [0, n) with a[i] >= x (n if none), for 1 <= n <= 2 * TOP, without
+// branches: a fixed number of halving steps.
+template <int TOP>
+__device__ __forceinline__ int lower_bound_bl(const int32_t* a, int n, int32_t x) {
+  static_assert(TOP > 0 && (TOP & (TOP - 1)) == 0, "the halving steps must be powers of two");
+  int lo = 0;
+#pragma unroll
+  for (int h = TOP; h >= 1; h >>= 1) {
+    const int idx = (lo + h < n ? lo + h : n) - 1;
+    lo = (lo + h <= n && a[idx] < x) ? lo + h : lo;
+  }
+  return lo;
+}
+
+// The k-th (0-based) set bit of an NW-word row, without branches.
+template <int NW>
+__device__ __forceinline__ int select_row(const uint64_t* row, int k) {
+  if constexpr (NW == 1) {
+    return select64(row[0], k);
+  } else {
+    int base = 0;
+    uint64_t word = row[0];
+    bool found = false;
+#pragma unroll
+    for (int w = 0; w < NW; ++w) {
+      const uint64_t v = row[w];
+      const int pc = __popcll(v);
+      const bool here = !found && k < pc;
+      word = here ? v : word;
+      base = here ? w * 64 : base;
+      k -= (!found && !here) ? pc : 0;
+      found = found || here;
+    }
+    return base + select64(word, k);
+  }
+}
+
 // Position of the j-th (0-based) set bit of an NW-word row.
 template <int NW>
 __device__ __forceinline__ int select_bit(const uint64_t* row, int j) {
@@ -185,6 +242,10 @@ static __device__ __forceinline__ void build_local_rows(const int32_t* adj, cons
   }
 }
 
+constexpr int HEAVY_BITS = 24;  // an item whose candidate set has this many members is
+                                // run by the whole warp instead of one lane (k >= 6)
+constexpr int HEAVY_SLOTS = 32;
+
 // The per-task words of a warp (shared memory).
 struct TaskWords {
   unsigned long long* range;  // item (or position) range: next | end << 32
@@ -192,6 +253,7 @@ struct TaskWords {
   int* busy;                  // serialises donations
   int* hn;                    // deferred heavy items
   int* heavy;                 // their item indices
+  uint64_t* stk = nullptr;    // the warp's walk stack (WalkR), where the kernel has one
 };
 
 // Per-lane clique counts by size (the fused count of every k up to K): c[s] = s-cliques.
@@ -223,11 +285,14 @@ template <int K, int NW, bool MULTI, int LEV0>
 struct Walk {
   static constexpr int D = K - LEV0 > 0 ? K - LEV0 : 1;
   Bits<NW> st[D];
+  const uint64_t* rows = nullptr;  // the local bitmap rows of the walk's root
   int top = -1;
   unsigned live = 0u;
 
-  // S: the candidates for vertex LEV0.
-  __device__ __forceinline__ void start(const Bits<NW>& S, Acc<K>& acc, unsigned long long& cnt) {
+  // S: the candidates for vertex LEV0, rows: the root's local bitmap rows.
+  __device__ __forceinline__ void start(const Bits<NW>& S, const uint64_t* root_rows, Acc<K>& acc,
+                                        unsigned long long& cnt) {
+    rows = root_rows;
     const int p = popc(S);
     if constexpr (MULTI) {
       acc.c[LEV0] += (unsigned long long)p;
@@ -249,8 +314,10 @@ struct Walk {
     }
   }
 
+  __device__ __forceinline__ void flush(Acc<K>&) {}
+
   // Expands one node of this lane's walk (top >= 0).
-  __device__ __forceinline__ void step(const uint64_t* __restrict__ rows, Acc<K>& acc, unsigned long long& cnt) {
+  __device__ __forceinline__ void step(Acc<K>& acc, unsigned long long& cnt) {
     if constexpr (LEV0 < K) {
       const int j = top;
       Bits<NW> cur;
@@ -316,6 +383,123 @@ struct CheckState {
   unsigned iter = 0u;
 };
 
+// The walk as the index kernel runs it: the top set in registers, the entries below it in
+// shared memory (stk: [entry][word][lane] u64 words of the warp, D - 1 entries), `live` bit j
+// set while entry j holds members, and the fused counts in separate scalars. One step is
+// branch-free: it reads the parent entry while the row of x loads and picks the next top set
+// with selects, so a lane's choice between going down, staying and going up never splits the
+// warp (a step is a chain of dependent operations: it costs the same for one lane or 32).
+template <int K, int NW, bool MULTI, int LEV0>
+struct WalkR {
+  static constexpr int D = K - LEV0 > 0 ? K - LEV0 : 1;
+  static_assert(!MULTI || D <= 4, "fused counts keep four level counters");
+  uint64_t* stk = nullptr;
+  const uint64_t* rows = nullptr;
+  Bits<NW> cur;
+  int top = -1;
+  unsigned live = 0u;
+  unsigned long long q0 = 0, q1 = 0, q2 = 0, q3 = 0;  // fused: counts at LEV0 + 1 + q
+
+  // S: the candidates for vertex LEV0, root_rows: the root's local bitmap rows.
+  __device__ __forceinline__ void start(const Bits<NW>& S, const uint64_t* root_rows, Acc<K>& acc,
+                                        unsigned long long& cnt) {
+    rows = root_rows;
+    const int p = popc(S);
+    bool go = false;
+    if constexpr (MULTI) {
+      acc.c[LEV0] += (unsigned long long)p;
+      if constexpr (LEV0 < K) go = p >= 2;
+    } else {
+      if constexpr (LEV0 == K) cnt += (unsigned long long)p;
+      else go = p >= K - LEV0 + 1;
+    }
+    if (go) {
+      cur = S;
+      top = 0;
+      live = 0u;
+    }
+  }
+
+  // Expands one node (top >= 0).
+  __device__ __forceinline__ void step(Acc<K>& /*acc*/, unsigned long long& cnt) {
+    if constexpr (LEV0 < K) {
+      const int lane = lane_id();
+      const int j = top;
+      int x = 0;
+      bool found = false;
+      Bits<NW> rest;
+#pragma unroll
+      for (int w = 0; w < NW; ++w) {
+        const uint64_t v = cur.w[w];
+        const bool here = !found && v != 0ull;
+        x = here ? w * 64 + __ffsll((long long)v) - 1 : x;
+        rest.w[w] = here ? (v & (v - 1ull)) : v;
+        found = found || here;
+      }
+      const unsigned below = live & ((1u << j) - 1u);
+      const int tgt = below ? 31 - __clz((int)below) : -1;
+      Bits<NW> par;
+      if constexpr (D >= 2) {
+        const int ti = tgt < 0 ? 0 : tgt;
+#pragma unroll
+        for (int w = 0; w < NW; ++w) par.w[w] = stk[(ti * NW + w) * 32 + lane];
+      } else {
+#pragma unroll
+        for (int w = 0; w < NW; ++w) par.w[w] = 0ull;
+      }
+      Bits<NW> T;
+#pragma unroll
+      for (int w = 0; w < NW; ++w) T.w[w] = rest.w[w] & rows[x * NW + w];
+      const int pc = popc(T);
+      bool push;
+      if constexpr (MULTI) {
+        q0 += j == 0 ? (unsigned long long)pc : 0ull;
+        if constexpr (D > 1) q1 += j == 1 ? (unsigned long long)pc : 0ull;
+        if constexpr (D > 2) q2 += j == 2 ? (unsigned long long)pc : 0ull;
+        if constexpr (D > 3) q3 += j == 3 ? (unsigned long long)pc : 0ull;
+        push = LEV0 + j + 1 < K && pc >= 2;
+      } else {
+        cnt += LEV0 + j + 1 == K ? (unsigned long long)pc : 0ull;
+        push = LEV0 + j + 1 < K && pc >= K - LEV0 - j;
+        // members left at this entry need K - LEV0 - j more vertices above them
+        const bool keep = popc(rest) > K - LEV0 - j;
+#pragma unroll
+        for (int w = 0; w < NW; ++w) rest.w[w] = keep ? rest.w[w] : 0ull;
+      }
+      uint64_t any = 0ull;
+#pragma unroll
+      for (int w = 0; w < NW; ++w) any |= rest.w[w];
+      if constexpr (D >= 2) {
+        if (push && any) {
+#pragma unroll
+          for (int w = 0; w < NW; ++w) stk[(j * NW + w) * 32 + lane] = rest.w[w];
+        }
+      }
+#pragma unroll
+      for (int w = 0; w < NW; ++w) cur.w[w] = push ? T.w[w] : (any ? rest.w[w] : par.w[w]);
+      const unsigned live_up = tgt >= 0 ? (live & ~(1u << tgt)) : 0u;
+      live = push ? (any ? (live | (1u << j)) : live) : (any ? live : live_up);
+      top = push ? j + 1 : (any ? j : tgt);
+    }
+  }
+
+  // Adds the fused counts of the steps taken to acc.
+  __device__ __forceinline__ void flush(Acc<K>& acc) {
+    if constexpr (MULTI && LEV0 < K) {
+      acc.c[LEV0 + 1] += q0;
+      if constexpr (D > 1) acc.c[LEV0 + 2] += q1;
+      if constexpr (D > 2) acc.c[LEV0 + 3] += q2;
+      if constexpr (D > 3) acc.c[LEV0 + 4] += q3;
+      q0 = q1 = q2 = q3 = 0ull;
+    }
+  }
+};
+
+// Shared-memory words a warp's WalkR stack needs (entries below the top).
+__host__ __device__ constexpr int walk_stack_words(int K, int NW, int LEV0) {
+  return (K - LEV0 > 1 ? K - LEV0 - 1 : 0) * NW * 32;
+}
+
 __device__ __forceinline__ unsigned lanemask_lt() {
   unsigned m;
   asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
@@ -323,31 +507,43 @@ __device__ __forceinline__ unsigned lanemask_lt() {
 }
 
 // The warp's loop over the items of tw.range: idle lanes take items (start_item(i) gives a
-// lane item i), walking lanes expand one node each. Lane 0 decides on donations from the
-// counters it sampled at its previous check (the loads stay in flight meanwhile): after every
-// refill that leaves items in the range, and every CHECK_EVERY iterations, where it also
-// takes a new sample; range_maybe_donate then splits the range. Items split off that no
-// queue slot took are run after the range. Returns when every item is done.
-template <int K, int NW, bool MULTI, int LEV0, class StartFn>
-__device__ __forceinline__ void lockstep_items(const LBArgs& lb, const TaskWords& tw, Walk<K, NW, MULTI, LEV0>& wk,
-                                               StartFn&& start_item, const uint64_t* rows, Acc<K>& acc,
-                                               unsigned long long& cnt, int root, long long t_start, int cost_tail,
-                                               int min_items, int level, const int* path, bool eager,
-                                               CheckState& cs) {
+// lane item i), walking lanes expand one node each. Lane 0 decides on donations without a
+// blocking load: from the counters it sampled at its previous check (loads that stay in
+// flight meanwhile), the items it knows are left, and the task's age in SM clock cycles
+// (two per nanosecond of donate_after_ns); it decides after every refill that leaves items in
+// the range and every CHECK_EVERY iterations, where it also takes a new sample, and then
+// range_split_donate splits the range. Items split off that no queue slot took are run after
+// the range. Returns when every item is done.
+// Lane 0: splits the rest of tw.range off as range_split_donate does when the sampled demand
+// asks for it, `left` items remain and the task is old enough (or eager); items that no queue
+// slot took are kept in [xb, xe).
+__device__ __forceinline__ void lockstep_donate(const LBArgs& lb, const TaskWords& tw, CheckState& cs, int left,
+                                                int need, int root, long long t_start, int cost_tail, int min_items,
+                                                int level, const int* path, bool eager, int& xb, int& xe) {
+  if (lb.hungry_trigger <= 0 || xe > xb || left < need) return;
+  if (cs.hungry - cs.queued < lb.hungry_trigger) return;
+  if (!eager && clock64() - t_start < 2ll * lb.donate_after_ns) return;
+  int ob = 0, oe = 0;
+  bool pushed = false;
+  if (range_split_donate(lb, tw.range, root, tw.don, tw.busy, ob, oe, cost_tail, min_items, level, path, &pushed)) {
+    xb = ob;
+    xe = oe;
+  }
+  if (pushed) ++cs.queued;  // this demand is served
+}
+
+// `src(i, wk, acc, cnt)` (a functor with a force-inlined call operator, so that the walk's
+// state stays in registers) starts item i on the calling lane.
+template <int K, class WK, class Src>
+__device__ __forceinline__ void lockstep_items(const LBArgs& lb, const TaskWords& tw, WK& wk, const Src& src,
+                                               Acc<K>& acc, unsigned long long& cnt, int root,
+                                               long long t_start, int cost_tail, int min_items, int level,
+                                               const int* path, bool eager, CheckState& cs) {
   const int lane = lane_id();
   bool open = true;
   int xb = 0, xe = 0;  // lane 0: split-off items to run after the range
-  // lane 0: split the range if the sampled demand asks for it
-  auto maybe_donate = [&]() {
-    if (lb.hungry_trigger > 0 && xe <= xb && (cs.hungry - cs.queued >= lb.hungry_trigger || eager)) {
-      int ob = 0, oe = 0;
-      if (range_maybe_donate(lb, tw.range, root, tw.don, t_start, tw.busy, ob, oe, cost_tail, min_items, level, path,
-                             eager)) {
-        xb = ob;
-        xe = oe;
-      }
-    }
-  };
+  const int need0 = min_items > 0 ? min_items : lb.min_split;
+  const int need = need0 > 2 ? need0 : 2;
   while (true) {
     const unsigned idle = __ballot_sync(FULL_MASK, wk.top < 0);
     if (open && idle != 0u && (idle == FULL_MASK || __popc(idle) >= REFILL_MIN)) {
@@ -359,10 +555,12 @@ __device__ __forceinline__ void lockstep_items(const LBArgs& lb, const TaskWords
       const int next = (int)(unsigned)old, end = (int)(unsigned)(old >> 32);
       if (wk.top < 0) {
         const int my = next + __popc(idle & lanemask_lt());
-        if (my < end) start_item(my);
+        if (my < end) src(my, wk, acc, cnt);
       }
       if (next + want < end) {
-        if (lane == 0) maybe_donate();
+        if (lane == 0)
+          lockstep_donate(lb, tw, cs, end - next - want, need, root, t_start, cost_tail, min_items, level, path, eager,
+                          xb, xe);
         __syncwarp();
       } else {
         const int has = __shfl_sync(FULL_MASK, xe > xb ? 1 : 0, 0);
@@ -383,12 +581,16 @@ __device__ __forceinline__ void lockstep_items(const LBArgs& lb, const TaskWords
       if (!open) break;
       continue;
     }
-    if (wk.top >= 0) wk.step(rows, acc, cnt);
+    if (wk.top >= 0) wk.step(acc, cnt);
     if (++cs.iter % CHECK_EVERY == 0u) {
       if (lane == 0) {
         atomicAdd(&lb.ctr->progress, (unsigned long long)CHECK_EVERY);
         if (lb.hungry_trigger > 0) {
-          if (open) maybe_donate();
+          if (open) {
+            const unsigned long long r = *reinterpret_cast<volatile unsigned long long*>(tw.range);
+            lockstep_donate(lb, tw, cs, (int)(unsigned)(r >> 32) - (int)(unsigned)r, need, root, t_start, cost_tail,
+                            min_items, level, path, eager, xb, xe);
+          }
           // read at the next check: the warp walks on while the loads complete
           cs.hungry = vload(&lb.ctr->hungry);
           cs.queued = vload(&lb.ctr->queued);
@@ -397,11 +599,63 @@ __device__ __forceinline__ void lockstep_items(const LBArgs& lb, const TaskWords
       __syncwarp();
     }
   }
+  wk.flush(acc);
 }
 
-constexpr int HEAVY_BITS = 24;  // an item whose candidate set has this many members is
-                                // run by the whole warp instead of one lane (k >= 6)
-constexpr int HEAVY_SLOTS = 32;
+// Item sources. Local edges of one root: item i is the edge (c1, c2) with c1 found in the
+// row prefix sE and c2 the matching bit of row c1; the walk starts at S = row[c1] & row[c2]
+// (vertex 4). For K >= 6 an item with HEAVY_BITS or more candidates is deferred to the heavy
+// list (run by the whole warp afterwards) while a slot is free.
+template <int K, int NW, bool MULTI>
+struct EdgeItems {
+  const uint64_t* rows;
+  const int32_t* sE;
+  int d;
+  int* hn;
+  int* heavy;
+  template <class WK>
+  __device__ __forceinline__ void operator()(int i, WK& wk, Acc<K>& acc, unsigned long long& cnt) const {
+    if constexpr (MULTI) acc.c[3] += 1ull;
+    // d + 1 <= 64 * NW + 1 entries: powers of two up to 64, 128 or 256 cover them
+    const int c1 = lower_bound_bl<(NW == 1 ? 64 : (NW == 2 ? 128 : 256))>(sE, d + 1, i + 1) - 1;
+    const int c2 = select_row<NW>(rows + c1 * NW, i - sE[c1]);
+    Bits<NW> S;
+#pragma unroll
+    for (int w = 0; w < NW; ++w) S.w[w] = rows[c1 * NW + w] & rows[c2 * NW + w];
+    if constexpr (K >= 6) {
+      const int p = popc(S);
+      if (p >= HEAVY_BITS) {
+        const int slot = atomicAdd(hn, 1);
+        if (slot < HEAVY_SLOTS) {
+          heavy[slot] = i;
+          if constexpr (MULTI) acc.c[4] += (unsigned long long)p;
+          return;
+        }
+      }
+    }
+    wk.start(S, rows, acc, cnt);
+  }
+};
+
+// Positions of a heavy item's candidate set S: position j picks vertex 4, c3 = the j-th
+// member of S, and the walk starts at S_{>c3} & row[c3] (vertex 5).
+template <int K, int NW, bool MULTI>
+struct PositionItems {
+  const uint64_t* rows;
+  Bits<NW> S;
+  template <class WK>
+  __device__ __forceinline__ void operator()(int j, WK& wk, Acc<K>& acc, unsigned long long& cnt) const {
+    const int c3 = select_row<NW>(S.w, j);
+    const int w3 = c3 >> 6;
+    const uint64_t above = (c3 & 63) == 63 ? 0ull : (~0ull << ((c3 & 63) + 1));
+    const uint64_t* rc = rows + c3 * NW;
+    Bits<NW> T;
+#pragma unroll
+    for (int w = 0; w < NW; ++w) T.w[w] = (w < w3 ? 0ull : (w == w3 ? (S.w[w] & above) : S.w[w])) & rc[w];
+    wk.start(T, rows, acc, cnt);
+  }
+};
+
 
 // Bitmap path for one task. Returns the k-cliques counted by this lane.
 template <int K, int NW, int M>
@@ -418,7 +672,6 @@ __device__ unsigned long long bitmap_task(const CliqueArgs& a, unsigned char* ws
   int* busy = reinterpret_cast<int*>(wsm + LY.busy);
   int* hn = reinterpret_cast<int*>(wsm + LY.hn);
   int* heavy = reinterpret_cast<int*>(wsm + LY.heavy);
-  const long long t_start = global_ns();
   // the donation checks' first sample is loaded while the bitmaps are built
   CheckState cs;
   if (lane == 0 && a.lb.hungry_trigger > 0) {
@@ -468,6 +721,7 @@ __device__ unsigned long long bitmap_task(const CliqueArgs& a, unsigned char* ws
   unsigned long long cnt = 0;
   if constexpr (K == 3) {
     // items are the rows: one popcount each, the lanes stay together
+    const long long t_start = global_ns();
     unsigned done = 0;
     while (true) {
       const int it = range_take(range);
@@ -494,26 +748,9 @@ __device__ unsigned long long bitmap_task(const CliqueArgs& a, unsigned char* ws
     const TaskWords tw{range, donations_left, busy, hn, heavy};
     Acc<K> unused;
     Walk<K, NW, false, 4> wk;
-    auto start_item = [&](int i) {
-      const int c1 = lower_bound(sE, 0, d + 1, i + 1) - 1;
-      const int c2 = select_bit<NW>(rows + c1 * NW, i - sE[c1]);
-      Bits<NW> S;
-#pragma unroll
-      for (int w = 0; w < NW; ++w) S.w[w] = rows[c1 * NW + w] & rows[c2 * NW + w];
-      if constexpr (K >= 6) {
-        // a large candidate set is run by the whole warp after the range
-        if (popc(S) >= HEAVY_BITS) {
-          const int slot = atomicAdd(hn, 1);
-          if (slot < HEAVY_SLOTS) {
-            heavy[slot] = i;
-            return;
-          }
-        }
-      }
-      wk.start(S, unused, cnt);
-    };
-    lockstep_items<K, NW, false, 4>(a.lb, tw, wk, start_item, rows, unused, cnt, root, t_start, 0, 0, 0, nullptr, false,
-                                    cs);
+    const EdgeItems<K, NW, false> items{rows, sE, d, hn, heavy};
+    const long long t_cyc = clock64();
+    lockstep_items<K>(a.lb, tw, wk, items, unused, cnt, root, t_cyc, 0, 0, 0, nullptr, false, cs);
     __syncwarp();
     if constexpr (K >= 6) {
       // heavy items: the members of S (clique vertex 4) are spread over the lanes; this
@@ -523,25 +760,14 @@ __device__ unsigned long long bitmap_task(const CliqueArgs& a, unsigned char* ws
         const int it = heavy[h];
         const int c1 = lower_bound(sE, 0, d + 1, it + 1) - 1;
         const int c2 = select_bit<NW>(rows + c1 * NW, it - sE[c1]);
-        Bits<NW> S;
+        PositionItems<K, NW, false> pos{rows, {}};
 #pragma unroll
-        for (int w = 0; w < NW; ++w) S.w[w] = rows[c1 * NW + w] & rows[c2 * NW + w];
+        for (int w = 0; w < NW; ++w) pos.S.w[w] = rows[c1 * NW + w] & rows[c2 * NW + w];
         __syncwarp();
-        if (lane == 0) *range = pack_range(0, popc(S));
+        if (lane == 0) *range = pack_range(0, popc(pos.S));
         __syncwarp();
         Walk<K, NW, false, 5> hw;
-        auto start_pos = [&](int j) {
-          const int c3 = select_bits<NW>(S, j);
-          const int w3 = c3 >> 6;
-          const uint64_t above = (c3 & 63) == 63 ? 0ull : (~0ull << ((c3 & 63) + 1));
-          const uint64_t* rc = rows + c3 * NW;
-          Bits<NW> T;
-#pragma unroll
-          for (int w = 0; w < NW; ++w) T.w[w] = (w < w3 ? 0ull : (w == w3 ? (S.w[w] & above) : S.w[w])) & rc[w];
-          hw.start(T, unused, cnt);
-        };
-        lockstep_items<K, NW, false, 5>(a.lb, tw, hw, start_pos, rows, unused, cnt, root, t_start, 0, INT_MAX, 0,
-                                        nullptr, false, cs);
+        lockstep_items<K>(a.lb, tw, hw, pos, unused, cnt, root, t_cyc, 0, INT_MAX, 0, nullptr, false, cs);
         __syncwarp();
       }
     }

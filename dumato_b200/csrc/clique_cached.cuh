@@ -147,20 +147,27 @@ __global__ void __launch_bounds__(256) index_build_kernel(GraphView g, const int
 // ---------------- counting on the index ----------------
 
 __host__ __device__ constexpr int stage_words(int M) { return M == 1 ? 512 : 1024; }
-constexpr int CHUNK_MAX = 16;  // roots claimed together
+constexpr int CHUNK_MAX = 16;     // roots claimed together
+constexpr int SMALL_ITEMS = 64;   // roots with at most this many local edges are batched
+constexpr int SMALL_WORDS = 512;  // ... from staging rounds of at most this many words
+constexpr int SMALL_ARRAYS = 4;   // batched entries: item offset, first word, out-degree, root
 
 // Shared memory of one warp: staged blocks | item prefix of the current root | task state |
 // bulk-copy barrier. At least warp_layout(M).total bytes, so that the list path (roots above
 // 256 out-neighbours), which keeps its state at warp_layout(M)'s offsets, can share it.
 struct CachedWarp {
-  int stage, E, range, don, busy, hn, heavy, mbar, total;
+  int stage, E, bat, stk, range, don, busy, hn, heavy, mbar, total;
 };
 
 __host__ __device__ constexpr CachedWarp cached_layout(int M) {
   CachedWarp w{};
   w.stage = 0;
   w.E = 8 * stage_words(M);
-  w.range = (w.E + 4 * (64 * M + 1) + 7) / 8 * 8;
+  // item prefix: of one root's rows, or of up to SMALL_WORDS staged words when small roots
+  // are batched
+  w.bat = w.E + 4 * (SMALL_WORDS + 1);
+  w.stk = (w.bat + 4 * SMALL_ARRAYS * (CHUNK_MAX + 1) + 15) / 16 * 16;
+  w.range = w.stk + 8 * walk_stack_words(INDEX_MAX_K, M, 4);
   w.don = w.range + 8;
   w.busy = w.don + 4;
   w.hn = w.busy + 4;
@@ -229,15 +236,10 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* mbar, unsigned parity) {
 // are hungry the upper part of the positions left is donated as (root, level 1, path = {it},
 // range).
 template <int K, int NW, bool MULTI>
-__device__ __forceinline__ unsigned long long heavy_run(const CachedArgs& a, const TaskWords& tw, const uint64_t* rows,
-                                                        const int32_t* sE, int d, int root, int it, int lo, int hi,
-                                                        bool eager, Acc<K>& acc, CheckState& cs) {
+__device__ __forceinline__ unsigned long long heavy_walk(const CachedArgs& a, const TaskWords& tw, const uint64_t* rows,
+                                                         const Bits<NW>& S, int root, int it, int lo, int hi,
+                                                         bool eager, Acc<K>& acc, CheckState& cs) {
   const int lane = lane_id();
-  const int c1 = lower_bound(sE, 0, d + 1, it + 1) - 1;
-  const int c2 = select_bit<NW>(rows + c1 * NW, it - sE[c1]);
-  Bits<NW> S;
-#pragma unroll
-  for (int w = 0; w < NW; ++w) S.w[w] = rows[c1 * NW + w] & rows[c2 * NW + w];
   const int p = popc(S);
   const int end = hi < 0 ? p : min(hi, p);
   __syncwarp();
@@ -247,23 +249,28 @@ __device__ __forceinline__ unsigned long long heavy_run(const CachedArgs& a, con
     *tw.busy = 0;
   }
   __syncwarp();
-  const long long t_start = lane == 0 ? global_ns() : 0;
+  const long long t_start = lane == 0 ? clock64() : 0;  // SM clock cycles
   const int path[1] = {it};
   unsigned long long cnt = 0;
-  Walk<K, NW, MULTI, 5> wk;
-  auto start_pos = [&](int j) {
-    const int c3 = select_bits<NW>(S, j);
-    const int w3 = c3 >> 6;
-    const uint64_t above = (c3 & 63) == 63 ? 0ull : (~0ull << ((c3 & 63) + 1));
-    const uint64_t* rc = rows + c3 * NW;
-    Bits<NW> T;
-#pragma unroll
-    for (int w = 0; w < NW; ++w) T.w[w] = (w < w3 ? 0ull : (w == w3 ? (S.w[w] & above) : S.w[w])) & rc[w];
-    wk.start(T, acc, cnt);
-  };
-  lockstep_items<K, NW, MULTI, 5>(a.c.lb, tw, wk, start_pos, rows, acc, cnt, root, t_start, p, 2, 1, path, eager, cs);
+  WalkR<K, NW, MULTI, 5> wk;
+  wk.stk = tw.stk;
+  const PositionItems<K, NW, MULTI> pos{rows, S};
+  lockstep_items<K>(a.c.lb, tw, wk, pos, acc, cnt, root, t_start, p, 2, 1, path, eager, cs);
   __syncwarp();
   return cnt;
+}
+
+// heavy_walk of item `it` of a root whose row prefix is sE.
+template <int K, int NW, bool MULTI>
+__device__ __forceinline__ unsigned long long heavy_run(const CachedArgs& a, const TaskWords& tw, const uint64_t* rows,
+                                                        const int32_t* sE, int d, int root, int it, int lo, int hi,
+                                                        bool eager, Acc<K>& acc, CheckState& cs) {
+  const int c1 = lower_bound(sE, 0, d + 1, it + 1) - 1;
+  const int c2 = select_bit<NW>(rows + c1 * NW, it - sE[c1]);
+  Bits<NW> S;
+#pragma unroll
+  for (int w = 0; w < NW; ++w) S.w[w] = rows[c1 * NW + w] & rows[c2 * NW + w];
+  return heavy_walk<K, NW, MULTI>(a, tw, rows, S, root, it, lo, hi, eager, acc, cs);
 }
 
 // Counts one root's task from its staged rows: level 0 runs items [b, e) (task_range
@@ -312,10 +319,10 @@ __device__ __forceinline__ unsigned long long staged_run(const CachedArgs& a, co
     *tw.hn = 0;
   }
   __syncwarp();
-  const long long t_start = lane == 0 ? global_ns() : 0;
   unsigned long long cnt = 0;
   if constexpr (K == 3) {
     // items are the rows: one popcount each, the lanes stay together
+    const long long t_start = global_ns();
     unsigned done = 0;
     int x;
     while ((x = range_take(tw.range)) >= 0) {
@@ -338,30 +345,11 @@ __device__ __forceinline__ unsigned long long staged_run(const CachedArgs& a, co
     __syncwarp();
     return cnt;
   } else {
-    Walk<K, NW, MULTI, 4> wk;
-    auto start_item = [&](int i) {
-      if constexpr (MULTI) acc.c[3] += 1ull;
-      const int c1 = lower_bound(sE, 0, d + 1, i + 1) - 1;
-      const int c2 = select_bit<NW>(rows + c1 * NW, i - sE[c1]);
-      Bits<NW> S;
-#pragma unroll
-      for (int w = 0; w < NW; ++w) S.w[w] = rows[c1 * NW + w] & rows[c2 * NW + w];
-      if constexpr (K >= 6) {
-        // a large candidate set is run by the whole warp after the range (heavy_run)
-        const int p = popc(S);
-        if (p >= HEAVY_BITS) {
-          const int slot = atomicAdd(tw.hn, 1);
-          if (slot < HEAVY_SLOTS) {
-            tw.heavy[slot] = i;
-            if constexpr (MULTI) acc.c[4] += (unsigned long long)p;
-            return;
-          }
-        }
-      }
-      wk.start(S, acc, cnt);
-    };
-    lockstep_items<K, NW, MULTI, 4>(a.c.lb, tw, wk, start_item, rows, acc, cnt, root, t_start, 0, 0, 0, nullptr, eager,
-                                    cs);
+    WalkR<K, NW, MULTI, 4> wk;
+    wk.stk = tw.stk;
+    const EdgeItems<K, NW, MULTI> items{rows, sE, d, tw.hn, tw.heavy};
+    const long long t_cyc = lane == 0 ? clock64() : 0;
+    lockstep_items<K>(a.c.lb, tw, wk, items, acc, cnt, root, t_cyc, 0, 0, 0, nullptr, eager, cs);
     __syncwarp();
     if constexpr (K >= 6) {
       const int nh = min(*tw.hn, HEAVY_SLOTS);
@@ -372,6 +360,142 @@ __device__ __forceinline__ unsigned long long staged_run(const CachedArgs& a, co
     }
     return cnt;
   }
+}
+
+// Items of the batched small roots of a staging round (small_batch): item g belongs to the
+// entry j with sO[j] <= g < sO[j + 1]; it is that entry's item e = g - sO[j], whose row c1
+// is the word r of the entry with E[r] <= E[sB[j]] + e < E[r + 1].
+template <int K, bool MULTI>
+struct BatchItems {
+  const uint64_t* srows;
+  const int32_t* E;
+  const int32_t* bat;  // sO | sB | sD | sR, CHUNK_MAX + 1 each
+  int ne;
+  int* hn;
+  int* heavy;
+  __device__ __forceinline__ void locate(int g, int& j, int& e, int& b0, Bits<1>& S) const {
+    const int32_t* sO = bat;
+    const int32_t* sB = bat + (CHUNK_MAX + 1);
+    const int32_t* sD = bat + 2 * (CHUNK_MAX + 1);
+    j = lower_bound_bl<16>(sO, ne + 1, g + 1) - 1;
+    e = g - sO[j];
+    b0 = sB[j];
+    const int target = E[b0] + e;
+    const int r = b0 + lower_bound_bl<64>(E + b0, sD[j] + 1, target + 1) - 1;
+    const int c2 = select64(srows[r], target - E[r]);
+    S.w[0] = srows[r] & srows[b0 + c2];
+  }
+  template <class WK>
+  __device__ __forceinline__ void operator()(int g, WK& wk, Acc<K>& acc, unsigned long long& cnt) const {
+    int j, e, b0;
+    Bits<1> S;
+    locate(g, j, e, b0, S);
+    if constexpr (MULTI) acc.c[3] += 1ull;
+    if constexpr (K >= 6) {
+      const int p = popc(S);
+      if (p >= HEAVY_BITS) {
+        const int slot = atomicAdd(hn, 1);
+        if (slot < HEAVY_SLOTS) {
+          heavy[slot] = g;
+          if constexpr (MULTI) acc.c[4] += (unsigned long long)p;
+          return;
+        }
+      }
+    }
+    wk.start(S, srows + b0, acc, cnt);
+  }
+};
+
+// Small roots of a staging round counted together. Entries [i0, i1) of the round are staged
+// (lane i holds entry i); those with rows of one word, a whole root (no part or donated range)
+// and at most SMALL_ITEMS local edges form one item space: the exclusive prefix E of the
+// popcounts of every staged word gives each entry's items, an entry's items follow the
+// items of the batched entries before it, and a lane maps item g to its entry (a search over
+// the entries' item offsets), its row c1 (a search over E within the entry) and c2 (a bit
+// select). One lockstep walk then covers all of them, so a root of a few items costs a few
+// lanes of one refill rather than a pass of the whole warp. The combined range is not
+// donated (a donation names one root); heavy items still donate their positions (level 1).
+// Returns the mask of the entries counted here.
+template <int K, bool MULTI>
+__device__ __forceinline__ unsigned small_batch(const CachedArgs& a, const TaskWords& tw, const uint64_t* srows,
+                                                int32_t* E, int32_t* bat, int i0, int i1, int root, int d,
+                                                uint32_t units, uint32_t rspos, int part, Acc<K>& acc,
+                                                unsigned long long& cnt, CheckState& cs) {
+  const int lane = lane_id();
+  const bool in_round = lane >= i0 && lane < i1;
+  const bool cand = in_round && units > 0 && d >= 2 && d <= 64 && (part & ~PART_EAGER) == 0;
+  if (__popc(__ballot_sync(FULL_MASK, cand)) < 2) return 0u;
+  // E over the round's staged words
+  const int W = (int)(2u * __shfl_sync(FULL_MASK, rspos + units, i1 - 1));
+  if (W > SMALL_WORDS) return 0u;
+  int carry = 0;
+  for (int w0 = 0; w0 < W; w0 += 32) {
+    const int w = w0 + lane;
+    const int pc = w < W ? __popcll(srows[w]) : 0;
+    int s = pc;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(FULL_MASK, s, o);
+      if (lane >= o) s += y;
+    }
+    if (w < W) E[w] = carry + s - pc;
+    carry += __shfl_sync(FULL_MASK, s, 31);
+  }
+  if (lane == 0) E[W] = carry;
+  __syncwarp();
+  const int base = (int)(2u * rspos);
+  const int n_items = cand ? E[base + d] - E[base] : 0;
+  const bool small = cand && n_items <= SMALL_ITEMS;
+  const unsigned done = __ballot_sync(FULL_MASK, small);
+  if (__popc(done) < 2) return 0u;
+  // item offsets of the batched entries (others hold no items), relative to i0
+  const int mine = small ? n_items : 0;
+  int s = mine;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(FULL_MASK, s, o);
+    if (lane >= o) s += y;
+  }
+  const int before = s - mine - __shfl_sync(FULL_MASK, s - mine, i0);  // exclusive, from entry i0
+  const int total = __shfl_sync(FULL_MASK, s, i1 - 1) - __shfl_sync(FULL_MASK, s - mine, i0);
+  const int ne = i1 - i0;
+  int32_t* sO = bat;
+  int32_t* sB = bat + (CHUNK_MAX + 1);
+  int32_t* sD = bat + 2 * (CHUNK_MAX + 1);
+  int32_t* sR = bat + 3 * (CHUNK_MAX + 1);
+  if (in_round) {
+    sO[lane - i0] = before;
+    sB[lane - i0] = base;
+    sD[lane - i0] = d;
+    sR[lane - i0] = root;
+  }
+  if (lane == 0) {
+    sO[ne] = total;
+    *tw.range = pack_range(0, total);
+    *tw.don = a.c.lb.max_donations;
+    *tw.busy = 0;
+    *tw.hn = 0;
+  }
+  __syncwarp();
+  if (total > 0) {
+    WalkR<K, 1, MULTI, 4> wk;
+    wk.stk = tw.stk;
+    const BatchItems<K, MULTI> items{srows, E, bat, ne, tw.hn, tw.heavy};
+    const long long t_cyc = lane == 0 ? clock64() : 0;
+    lockstep_items<K>(a.c.lb, tw, wk, items, acc, cnt, 0, t_cyc, 0, INT_MAX, 0, nullptr, false, cs);
+    __syncwarp();
+    if constexpr (K >= 6) {
+      const int nh = min(*tw.hn, HEAVY_SLOTS);
+      for (int h = 0; h < nh; ++h) {
+        int j, e, b0;
+        Bits<1> S;
+        items.locate(tw.heavy[h], j, e, b0, S);
+        cnt += heavy_walk<K, 1, MULTI>(a, tw, srows + b0, S, sR[j], e, 0, -1, false, acc, cs);
+      }
+    }
+  }
+  __syncwarp();
+  return done;
 }
 
 template <int K, int M, bool MULTI>
@@ -460,10 +584,11 @@ __global__ void __launch_bounds__(256, cached_min_blocks<M>()) clique_cached_ker
   uint4* stage = reinterpret_cast<uint4*>(wsm + LY.stage);
   const uint64_t* srows = reinterpret_cast<const uint64_t*>(wsm + LY.stage);
   int32_t* sE = reinterpret_cast<int32_t*>(wsm + LY.E);
+  int32_t* sBat = reinterpret_cast<int32_t*>(wsm + LY.bat);
   uint64_t* mbar = reinterpret_cast<uint64_t*>(wsm + LY.mbar);
   TaskWords tw{reinterpret_cast<unsigned long long*>(wsm + LY.range), reinterpret_cast<int*>(wsm + LY.don),
                reinterpret_cast<int*>(wsm + LY.busy), reinterpret_cast<int*>(wsm + LY.hn),
-               reinterpret_cast<int*>(wsm + LY.heavy)};
+               reinterpret_cast<int*>(wsm + LY.heavy), reinterpret_cast<uint64_t*>(wsm + LY.stk)};
   if constexpr (TMA) {
     if (lane == 0) mbar_init(mbar);
     __syncwarp();
@@ -565,7 +690,15 @@ __global__ void __launch_bounds__(256, cached_min_blocks<M>()) clique_cached_ker
           if (lane == 0) set_err(a.c.lb.ctr, ERR_TIMEOUT);
         }
       }
+      unsigned batched = 0u;
+      if constexpr (K >= 4) {
+        if (!donated && !a.c.per_root) {
+          batched = small_batch<K, MULTI>(a, tw, srows, sE, sBat, i0, i1, root, d, units, rspos, part, acc, cnt, cs);
+          ntasks += __popc(batched);
+        }
+      }
       for (int i = i0; i < i1; ++i) {
+        if ((batched >> i) & 1u) continue;
         const int r = __shfl_sync(FULL_MASK, root, i);
         const int di = __shfl_sync(FULL_MASK, d, i);
         const uint32_t ui = __shfl_sync(FULL_MASK, units, i);

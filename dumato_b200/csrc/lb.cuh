@@ -321,24 +321,17 @@ __device__ __forceinline__ int split_mid(int next, int end, int cost_tail) {
   return next + max(1, min(end - next - 1, x));
 }
 
-// If more warps are hungry than tasks are queued and the task has run longer than
-// donate_after_ns, splits the upper
-// half of the remaining range off and enqueues it (with cost_tail > 0, item i is taken to
-// cost cost_tail - i and the split halves the remaining cost instead of the item count; a
-// range is split only with at least min_items (default lb.min_split) left). Returns true when the queue was full:
-// the split-off items [ob, oe) then belong to the caller, who must run them itself
-// (lanes that find the range empty have already moved the cursor past `mid`, so the split
-// cannot simply be undone). `busy` serialises donations of one warp.
-__device__ __forceinline__ bool range_maybe_donate(const LBArgs& lb, unsigned long long* range, int root,
-                                                   int* donations_left, long long task_start, int* busy, int& ob,
-                                                   int& oe, int cost_tail = 0, int min_items = 0, int level = 0,
-                                                   const int* path = nullptr, bool eager = false) {
-  if (lb.hungry_trigger <= 0) return false;
+// Splits the upper part of the remaining items [next, end) of a task's range off and
+// enqueues it as (root, [mid, end)) at `level` with `path` (with cost_tail > 0, item i is
+// taken to cost cost_tail - i and the split halves the remaining cost instead of the item
+// count; a range is split only with at least min_items (default lb.min_split) left). Returns
+// true when the queue was full: the split-off items [ob, oe) then belong to the caller, who
+// must run them itself (lanes that find the range empty have already moved the cursor past
+// `mid`, so the split cannot simply be undone). `busy` serialises donations of one warp.
+__device__ __forceinline__ bool range_split_donate(const LBArgs& lb, unsigned long long* range, int root,
+                                                   int* donations_left, int* busy, int& ob, int& oe, int cost_tail,
+                                                   int min_items, int level, const int* path, bool* donated = nullptr) {
   if (*reinterpret_cast<volatile int*>(donations_left) <= 0) return false;
-  // demand: hungry warps not yet served by a queued task
-  const int hungry = vload(&lb.ctr->hungry);
-  if (hungry - vload(&lb.ctr->queued) < lb.hungry_trigger) return false;
-  if (!eager && global_ns() - task_start < lb.donate_after_ns) return false;
   if (atomicCAS(busy, 0, 1) != 0) return false;
   bool own = false;
   unsigned long long cur = *reinterpret_cast<volatile unsigned long long*>(range);
@@ -358,6 +351,7 @@ __device__ __forceinline__ bool range_maybe_donate(const LBArgs& lb, unsigned lo
       atomicSub(donations_left, 1);
       atomicAdd(&lb.ctr->donations, 1ull);
       if (level > 0) atomicAdd(&lb.ctr->prefix_donations, 1ull);
+      if (donated) *donated = true;
     } else {
       atomicSub(&lb.ctr->pending, 1);
       ob = mid;
@@ -368,6 +362,21 @@ __device__ __forceinline__ bool range_maybe_donate(const LBArgs& lb, unsigned lo
   }
   atomicExch(busy, 0);
   return own;
+}
+
+// If more warps are hungry than tasks are queued and the task has run longer than
+// donate_after_ns (or `eager`), splits the range as range_split_donate does.
+__device__ __forceinline__ bool range_maybe_donate(const LBArgs& lb, unsigned long long* range, int root,
+                                                   int* donations_left, long long task_start, int* busy, int& ob,
+                                                   int& oe, int cost_tail = 0, int min_items = 0, int level = 0,
+                                                   const int* path = nullptr, bool eager = false) {
+  if (lb.hungry_trigger <= 0) return false;
+  if (*reinterpret_cast<volatile int*>(donations_left) <= 0) return false;
+  // demand: hungry warps not yet served by a queued task
+  const int hungry = vload(&lb.ctr->hungry);
+  if (hungry - vload(&lb.ctr->queued) < lb.hungry_trigger) return false;
+  if (!eager && global_ns() - task_start < lb.donate_after_ns) return false;
+  return range_split_donate(lb, range, root, donations_left, busy, ob, oe, cost_tail, min_items, level, path);
 }
 
 // Demand test shared by the donation paths (lane 0): hungry warps outnumber queued tasks by
