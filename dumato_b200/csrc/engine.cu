@@ -52,6 +52,8 @@ struct Workspace {
   // learned schedule: MLP parameters, scratch and output task list
   float* d_params = nullptr;
   size_t params_cap = 0;
+  uint64_t params_uid = 0, params_version = 0;  // the predictor version held in d_params
+  int* h_hdr = nullptr;                          // pinned pair for the schedule's header
   void* d_sched = nullptr;
   size_t sched_cap = 0;
   int32_t* d_sroots = nullptr;
@@ -313,6 +315,7 @@ static void free_workspace(Workspace& w) {
   if (w.k0) cudaEventDestroy(w.k0);
   if (w.k1) cudaEventDestroy(w.k1);
   if (w.h_init) cudaFreeHost(w.h_init);
+  if (w.h_hdr) cudaFreeHost(w.h_hdr);
   if (w.h_out) cudaFreeHost(w.h_out);
   w = Workspace();
 }
@@ -703,9 +706,14 @@ static int learned_device(dm_graph* g, DeviceSlot* s, const dm_opts* o, int k, b
   if (with_desc &&
       (rc = ensure_ws_bytes(reinterpret_cast<void**>(&ws.d_sdesc), &ws.sdesc_cap, sizeof(RootDesc) * cap)))
     return rc;
+  if (!ws.h_hdr) DM_CUDA(cudaMallocHost(&ws.h_hdr, 2 * sizeof(int)));
+  uint64_t uid = 0, version = 0;
+  predictor_key(o->predictor, &uid, &version);
   SchedIO io;
   io.feat = s->d_feat[eng];
   io.params = ws.d_params;
+  io.params_current = uid != 0 && ws.params_uid == uid && ws.params_version == version;
+  io.h_hdr = ws.h_hdr;
   io.roots = in_roots;
   io.orig = clique ? s->d_orig : nullptr;
   io.n_in = n_in;
@@ -718,7 +726,10 @@ static int learned_device(dm_graph* g, DeviceSlot* s, const dm_opts* o, int k, b
   io.out_desc = with_desc ? ws.d_sdesc : nullptr;
   io.odeg = s->dg.d_odeg;
   io.boff = with_desc ? s->d_boff : nullptr;
+  ws.params_uid = 0;  // until the call has written this version's parameters
   if ((rc = learned_schedule_device(o->predictor, io, ctx, n))) return rc;
+  ws.params_uid = uid;
+  ws.params_version = version;
   *roots = ws.d_sroots;
   *parts = ws.d_sparts;
   if (desc) *desc = with_desc ? ws.d_sdesc : nullptr;

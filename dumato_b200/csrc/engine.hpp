@@ -102,7 +102,9 @@ constexpr int PART_EAGER = 1 << 30;
 // The learned schedule on the device (predictor.cu): inputs, scratch and outputs.
 struct SchedIO {
   const float* feat = nullptr;       // n x 6 base features by original id
-  float* params = nullptr;           // MLP parameters (written by the call)
+  float* params = nullptr;           // MLP parameters on the device
+  bool params_current = false;       // params already hold this predictor's version
+  int* h_hdr = nullptr;              // pinned: the schedule's task count and error flag
   const int32_t* roots = nullptr;    // n_in input entries
   const int32_t* orig = nullptr;     // rank -> original id (cliques), else null
   int n_in = 0, k = 0, warps = 1, cap = 0;

@@ -491,8 +491,9 @@ int learned_schedule_device(const void* pv, const SchedIO& io, LaunchCtx& ctx, i
   // the scratch header (total, n_out, err, bins) starts at zero
   DM_CUDA(cudaMemsetAsync(io.scratch, 0, (size_t)(reinterpret_cast<char*>(a.cost) - reinterpret_cast<char*>(io.scratch)),
                           ctx.stream));
-  DM_CUDA(cudaMemcpyAsync(io.params, p->params.data(), sizeof(float) * MLP_NP,
-                          cudaMemcpyHostToDevice, ctx.stream));
+  if (!io.params_current)
+    DM_CUDA(cudaMemcpyAsync(io.params, p->params.data(), sizeof(float) * MLP_NP, cudaMemcpyHostToDevice,
+                            ctx.stream));
   const unsigned grid = (unsigned)std::max(1, (io.n_in + 255) / 256);
   sched_predict_kernel<<<grid, 256, 0, ctx.stream>>>(a);
   sched_parts_kernel<<<grid, 256, 0, ctx.stream>>>(a);
@@ -500,7 +501,8 @@ int learned_schedule_device(const void* pv, const SchedIO& io, LaunchCtx& ctx, i
   sched_scatter_kernel<<<grid, 256, 0, ctx.stream>>>(a);
   ctx.launches += 4;
   DM_CUDA(cudaGetLastError());
-  int hdr[2] = {0, 0};
+  // the task count and the error flag, through a page-locked pair (asynchronous copies)
+  int* hdr = io.h_hdr;
   DM_CUDA(cudaMemcpyAsync(&hdr[0], a.n_out, sizeof(int), cudaMemcpyDeviceToHost, ctx.stream));
   DM_CUDA(cudaMemcpyAsync(&hdr[1], a.err, sizeof(int), cudaMemcpyDeviceToHost, ctx.stream));
   DM_CUDA(cudaStreamSynchronize(ctx.stream));
