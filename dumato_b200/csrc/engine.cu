@@ -580,6 +580,14 @@ static int ensure_deg_order(dm_graph* g, DeviceSlot* s, cudaStream_t st) {
   return DM_OK;
 }
 
+// Entries of a root in the plain task list of the index: about d^2 / 256 for 32 to 64
+// out-neighbours (its local edges, the items, number up to d(d-1)/2), else 1. Wider roots
+// stay whole: their heavy items already split below the first level (level-1 donations), and
+// parts would stage their large blocks once per part (measured on an R-MAT graph with roots
+// of 106-171 out-neighbours: 7-cliques 70 ms whole, 79 ms in 16 parts; roots of 48-59
+// out-neighbours on another R-MAT graph: 173 µs whole, 129 µs in parts).
+static int split_parts(int d) { return d < 32 || d > 64 ? 1 : std::max(1, (d * d + 128) / 256); }
+
 static RootDesc root_desc(const dm_graph* g, const DeviceSlot* /*s*/, int32_t r, int32_t part) {
   return RootDesc{r, (int32_t)(g->orow[r + 1] - g->orow[r]), g->idx_boff.empty() ? INDEX_NONE : g->idx_boff[r],
                   part};
@@ -608,11 +616,21 @@ static int ensure_index(dm_graph* g, DeviceSlot* s, LaunchCtx& ctx) {
     g->idx_boff.swap(boff);
     g->idx_units = total;
     g->idx_maxd = max_d;
-    g->idx_desc.assign((size_t)4 * n, 0);
+    // roots of 32 or more out-neighbours enter the list as split_parts(d) entries, each for
+    // an even share of the root's items: the warps dealt those entries start on the heaviest
+    // roots together instead of one warp walking each of them alone
+    g->idx_desc.clear();
+    g->idx_desc.reserve((size_t)4 * n);
     for (int32_t i = 0; i < n; ++i) {
-      const RootDesc rd = root_desc(g, s, g->deg_order[i], 0);
-      std::memcpy(g->idx_desc.data() + 4 * (size_t)i, &rd, sizeof(RootDesc));
+      const int32_t r = g->deg_order[i];
+      const int P = split_parts((int)(g->orow[r + 1] - g->orow[r]));
+      for (int q = 0; q < P; ++q) {
+        const RootDesc rd = root_desc(g, s, r, P > 1 ? (q | (P << 16)) : 0);
+        const int32_t* w = reinterpret_cast<const int32_t*>(&rd);
+        g->idx_desc.insert(g->idx_desc.end(), w, w + 4);
+      }
     }
+    g->idx_extra = (int32_t)(g->idx_desc.size() / 4 - (size_t)n);
     pin_host(g, g->idx_boff.data(), sizeof(uint32_t) * g->idx_boff.size());
     pin_host(g, g->idx_desc.data(), sizeof(int32_t) * g->idx_desc.size());
   }
@@ -633,7 +651,8 @@ static int ensure_index(dm_graph* g, DeviceSlot* s, LaunchCtx& ctx) {
   RootDesc* desc = nullptr;
   cudaError_t e = gbuf_alloc(&blocks, std::max<size_t>(bytes, 16));
   if (e == cudaSuccess) e = gbuf_alloc(reinterpret_cast<void**>(&d_boff), sizeof(uint32_t) * std::max(n, 1));
-  if (e == cudaSuccess) e = gbuf_alloc(reinterpret_cast<void**>(&desc), sizeof(RootDesc) * std::max(n, 1));
+  const size_t n_desc = g->idx_desc.size() / 4;
+  if (e == cudaSuccess) e = gbuf_alloc(reinterpret_cast<void**>(&desc), sizeof(RootDesc) * std::max<size_t>(n_desc, 1));
   if (e != cudaSuccess) {
     gbuf_free(blocks, ctx.device);
     gbuf_free(d_boff, ctx.device);
@@ -649,7 +668,8 @@ static int ensure_index(dm_graph* g, DeviceSlot* s, LaunchCtx& ctx) {
   s->index_state = 1;
   if (n) {
     DM_CUDA(cudaMemcpyAsync(d_boff, g->idx_boff.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice, ctx.stream));
-    DM_CUDA(cudaMemcpyAsync(desc, g->idx_desc.data(), sizeof(RootDesc) * n, cudaMemcpyHostToDevice, ctx.stream));
+    DM_CUDA(cudaMemcpyAsync(desc, g->idx_desc.data(), sizeof(RootDesc) * n_desc, cudaMemcpyHostToDevice,
+                            ctx.stream));
   }
   // roots with out-degree in [2, 256] are a contiguous range of the descending-degree order
   const int64_t lo = INDEX_MAX_DEGREE + 1 < (int64_t)g->cnt_ge.size() ? g->cnt_ge[INDEX_MAX_DEGREE + 1] : 0;
@@ -887,6 +907,8 @@ static int count_cliques_impl(dm_graph* g, int32_t k, const dm_opts* o, uint64_t
     }
   }
   const bool use_index = want_index && s->index_state == 1 && d_desc != nullptr;
+  // the plain task list on the index holds the parts of the split roots too (they lead it)
+  if (use_index && d_desc == s->d_desc_deg && n_roots > 0) n_roots += g->idx_extra;
   if (upto && (!use_index || max_d > INDEX_MAX_DEGREE || (o && o->subtree_counts))) return 1;
   CliqueLaunch L;
   L.k = k;
