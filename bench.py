@@ -361,6 +361,7 @@ def main():
     # each step, outside the events
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     fused_ms = []
+    fused_idle = []
     emb = 0
     launches = 0
     barrier()
@@ -374,6 +375,7 @@ def main():
             emb += c
             launches += nl
             fused_ms.append(coll[0][1].kernel_ms)
+            fused_idle.append(coll[0][1].idle_warp_fraction)
         barrier()
     t_total = sum(a.elapsed_time(b) for a, b in ev) / 1e3
     if world > 1:
@@ -435,10 +437,13 @@ def main():
     achieved = alg_bytes / kern_s / 1e9
     # DRAM bytes per launch from the committed ncu capture of this kernel and workload
     traffic = None
+    l2 = None
     prof = ROOT / "profiles" / "clique_chunglu18k_traffic.json"
     if prof.exists():
         try:
-            traffic = json.loads(prof.read_text()).get("dram_bytes_per_launch")
+            pj = json.loads(prof.read_text())
+            traffic = pj.get("dram_bytes_per_launch")
+            l2 = pj.get("l2")
         except Exception:
             traffic = None
 
@@ -466,12 +471,15 @@ def main():
                        "step": "one dm_count_cliques_upto(kmax=7) call: one launch counts k = 4..7",
                        "l2": "flushed before every step (256 MB write)"},
             "fused_time_to_count_ms": statistics.mean(fused_ms),
+            # the persistent launch's makespan is its duration; idle = warp time spent waiting
+            "load_balance": {"makespan_ms": statistics.mean(fused_ms),
+                             "idle_warp_fraction": statistics.mean(fused_idle)},
             "time_to_count_ms": {str(k): statistics.mean(per_k[k]) for k in KS},
             "embeddings_per_step": emb // max(args.steps, 1),
             "gpu_launches": launches,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
-                         "algorithmic_bytes_per_launch": alg_bytes,
+                         "algorithmic_bytes_per_launch": alg_bytes, "l2": l2,
                          "kernel": "clique_cached_kernel<7, 1, TMA, fused> (one launch per step)"},
             "e2e": {"value": e2e_value, "unit": "embeddings/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "steps": e2e_steps,
