@@ -580,13 +580,13 @@ static int ensure_deg_order(dm_graph* g, DeviceSlot* s, cudaStream_t st) {
   return DM_OK;
 }
 
-// Entries of a root in the plain task list of the index: about d^2 / 256 for 32 to 64
+// Entries of a root in the plain task list of the index: about d^2 / 256 for 20 to 64
 // out-neighbours (its local edges, the items, number up to d(d-1)/2), else 1. Wider roots
 // stay whole: their heavy items already split below the first level (level-1 donations), and
 // parts would stage their large blocks once per part (measured on an R-MAT graph with roots
 // of 106-171 out-neighbours: 7-cliques 70 ms whole, 79 ms in 16 parts; roots of 48-59
 // out-neighbours on another R-MAT graph: 173 µs whole, 129 µs in parts).
-static int split_parts(int d) { return d < 32 || d > 64 ? 1 : std::max(1, (d * d + 128) / 256); }
+static int split_parts(int d) { return d < 20 || d > 64 ? 1 : std::max(1, (d * d + 128) / 256); }
 
 static RootDesc root_desc(const dm_graph* g, const DeviceSlot* /*s*/, int32_t r, int32_t part) {
   return RootDesc{r, (int32_t)(g->orow[r + 1] - g->orow[r]), g->idx_boff.empty() ? INDEX_NONE : g->idx_boff[r],
