@@ -452,7 +452,20 @@ class Options:
     report: Optional[object] = None   # callable(dict), called every report_ms while a kernel runs
     report_ms: int = 0
 
+    def __setattr__(self, name, value):
+        object.__setattr__(self, name, value)
+        if name != "_c_cache":
+            object.__setattr__(self, "_c_cache", None)  # any change rebuilds the C struct
+
     def to_c(self) -> _Opts:
+        c = self.__dict__.get("_c_cache")
+        if c is not None:
+            return c
+        c = self._build_c()
+        object.__setattr__(self, "_c_cache", c)
+        return c
+
+    def _build_c(self) -> _Opts:
         st = None
         if self.subtree_counts is not None:
             if self.subtree_counts.dtype != np.uint64 or not self.subtree_counts.flags.c_contiguous:

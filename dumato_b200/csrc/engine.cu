@@ -124,16 +124,22 @@ static std::map<int, cudaStream_t> g_streams;
 static std::map<int, int> g_sms;
 
 int select_device(const dm_opts* o, LaunchCtx& ctx) {
-  int count = 0;
-  cudaError_t e = cudaGetDeviceCount(&count);
-  if (e != cudaSuccess || count == 0) {
-    cudaGetLastError();
-    return fail(DM_ENODEVICE, std::string("no usable CUDA device: ") + cudaGetErrorString(e));
+  // the device count is fixed for the process once it is known (a failed query is retried)
+  static std::atomic<int> known_count{0};
+  int count = known_count.load(std::memory_order_relaxed);
+  if (count == 0) {
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || count == 0) {
+      cudaGetLastError();
+      return fail(DM_ENODEVICE, std::string("no usable CUDA device: ") + cudaGetErrorString(e));
+    }
+    known_count.store(count, std::memory_order_relaxed);
   }
-  int dev = (o && o->device >= 0) ? o->device : -1;
-  if (dev < 0) DM_CUDA(cudaGetDevice(&dev));
+  int cur = -1;
+  DM_CUDA(cudaGetDevice(&cur));
+  int dev = (o && o->device >= 0) ? o->device : cur;
   if (dev >= count) return fail(DM_EINVAL, "device ordinal out of range");
-  DM_CUDA(cudaSetDevice(dev));
+  if (dev != cur) DM_CUDA(cudaSetDevice(dev));
   ctx.device = dev;
   std::lock_guard<std::mutex> lk(g_dev_mu);
   if (!g_sms.count(dev)) {
