@@ -323,9 +323,10 @@ def batched(dm, workloads, reps: int = 2):
 def e2e_upload_bytes(g) -> int:
     """Bytes one e2e step copies host -> device for a clique count on the index: the oriented
     CSR (n row starts, n degrees, rows padded to multiples of 4 ints), the descending-degree
-    root order (n ints) and the 1,152-byte counter block. The index, its block offsets and its
-    task list are built on the device from these. The DAG orients every edge from the lower
-    to the higher (degree, id) rank."""
+    root order (n ints), the index block offsets (n ints), the task list (16 bytes per entry:
+    one per root, or split_parts(d) for roots of 20..64 out-neighbours, as engine.cu builds
+    it) and the 1,152-byte counter block. The DAG orients every edge from the lower to the
+    higher (degree, id) rank."""
     u, v = g.edges()
     n = g.info().n_vertices
     deg = np.bincount(np.concatenate([u, v]), minlength=n)
@@ -334,7 +335,9 @@ def e2e_upload_bytes(g) -> int:
     lo = np.where(rank[u] < rank[v], u, v)
     od = np.bincount(lo, minlength=n)
     padded = max(int(((od + 3) // 4 * 4).sum()), 4)
-    return 4 * n + 4 * n + 4 * padded + 4 * n + 1152
+    split = (od >= 20) & (od <= 64)
+    parts = np.where(split, np.maximum(1, (od * od + 128) // 256), 1)
+    return 4 * n + 4 * n + 4 * padded + 4 * n + 4 * n + 16 * int(parts.sum()) + 1152
 
 
 def main():
@@ -427,8 +430,8 @@ def main():
         upload_ms.append(coll[0][1].prep_ms)  # the call uploads the graph and builds the index
     n, m = info.n_vertices, info.n_edges
     # padded oriented CSR (row starts, degrees, adjacency padded to 4-int rows), the root
-    # order and the per-call counter block (the index and its tables are built on the
-    # device); the counter block is read back per call
+    # order, the clique index's block offsets and task list (the index itself is built on
+    # the device), and the per-call counter block; the counter block is read back per call
     h2d = e2e_upload_bytes(g)
     d2h = 1152
     e2e_t = e2e_ms / 1e3

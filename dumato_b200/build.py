@@ -22,7 +22,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
           "-I", str(PKG.parent / "include"), "-I", str(CSRC)]
 LIB_SOURCES = ["graph.cpp", "dictionary.cpp", "engine.cu", "clique.cu", "clique_k7_8.cu", "clique_k9.cu",
-               "clique_k10.cu", "clique_k11.cu", "clique_k12.cu", "motif.cu", "predictor.cu", "noalloc.cu", "batch.cu", "ingest.cu", "near_clique.cu", "index_tables.cu"]
+               "clique_k10.cu", "clique_k11.cu", "clique_k12.cu", "motif.cu", "predictor.cu", "noalloc.cu", "batch.cu", "ingest.cu", "near_clique.cu"]
 CLI_SOURCES = {"clique": "cli_clique.cpp", "motifs": "cli_motifs.cpp", "near_clique": "cli_near_clique.cpp"}
 
 

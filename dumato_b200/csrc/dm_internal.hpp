@@ -70,6 +70,7 @@ struct dm_graph {
   std::vector<int32_t> deg_order;     // ranks by descending DAG out-degree (stable in rank)
   std::vector<int64_t> cnt_ge;        // cnt_ge[d] = ranks with out-degree >= d
   std::vector<uint32_t> idx_boff;     // clique-index block offset per rank (16-byte units)
+  std::vector<int32_t> idx_desc;      // task list of deg_order on the index, 4 ints per entry
   int32_t idx_extra = 0;              // entries beyond one per root (roots split into parts)
   uint64_t idx_units = 0;             // 16-byte units of the whole index
   int32_t idx_maxd = 0;               // largest out-degree with a block

@@ -111,7 +111,6 @@ struct DeviceSlot {
   int index_state = 0;              // 0 not built, 1 built, -1 over the memory budget
   void* d_blocks = nullptr;
   uint32_t* d_boff = nullptr;
-  void* d_index_tmp = nullptr;      // scratch of the device-built index tables
   size_t index_bytes = 0;
   RootDesc* d_desc_deg = nullptr;   // task list of the descending-degree order (index counting)
   // learned scheduler inputs on the device: base features per engine (0 = motifs, 1 =
@@ -515,7 +514,7 @@ void release_device_graphs(dm_graph* g) {
       for (void* p : {(void*)s->dg.d_row, (void*)s->dg.d_deg, (void*)s->dg.d_adj, (void*)s->dg.d_orow,
                       (void*)s->dg.d_odeg, (void*)s->dg.d_oadj, (void*)s->d_deg_order, (void*)s->d_up_order,
                       s->d_blocks, (void*)s->d_boff, (void*)s->d_desc_deg, (void*)s->d_feat[0], (void*)s->d_feat[1],
-                      (void*)s->d_orig, s->d_index_tmp})
+                      (void*)s->d_orig})
         gbuf_free(p, dv);
       {
         std::lock_guard<std::mutex> lk(g_dev_mu);
@@ -587,6 +586,14 @@ static int ensure_deg_order(dm_graph* g, DeviceSlot* s, cudaStream_t st) {
   return DM_OK;
 }
 
+// Entries of a root in the plain task list of the index: about d^2 / 256 for 20 to 64
+// out-neighbours (its local edges, the items, number up to d(d-1)/2), else 1. Wider roots
+// stay whole: their heavy items already split below the first level (level-1 donations), and
+// parts would stage their large blocks once per part (measured on an R-MAT graph with roots
+// of 106-171 out-neighbours: 7-cliques 70 ms whole, 79 ms in 16 parts; roots of 48-59
+// out-neighbours on another R-MAT graph: 173 µs whole, 129 µs in parts).
+static int split_parts(int d) { return d < 20 || d > 64 ? 1 : std::max(1, (d * d + 128) / 256); }
+
 static RootDesc root_desc(const dm_graph* g, const DeviceSlot* /*s*/, int32_t r, int32_t part) {
   return RootDesc{r, (int32_t)(g->orow[r + 1] - g->orow[r]), g->idx_boff.empty() ? INDEX_NONE : g->idx_boff[r],
                   part};
@@ -615,14 +622,23 @@ static int ensure_index(dm_graph* g, DeviceSlot* s, LaunchCtx& ctx) {
     g->idx_boff.swap(boff);
     g->idx_units = total;
     g->idx_maxd = max_d;
-    // roots of 20..64 out-neighbours enter the task list as index_split_parts(d) entries,
-    // each for an even share of the root's items: the warps dealt those entries start on the
-    // heaviest roots together instead of one warp walking each of them alone. The list and
-    // the block offsets are built on the device (index_tables_build); the host keeps the
-    // offsets for the task lists of the other schedules and the number of extra entries.
-    int64_t extra = 0;
-    for (int32_t r = 0; r < n; ++r) extra += index_split_parts((int)(g->orow[r + 1] - g->orow[r])) - 1;
-    g->idx_extra = (int32_t)extra;
+    // roots of 32 or more out-neighbours enter the list as split_parts(d) entries, each for
+    // an even share of the root's items: the warps dealt those entries start on the heaviest
+    // roots together instead of one warp walking each of them alone
+    g->idx_desc.clear();
+    g->idx_desc.reserve((size_t)4 * n);
+    for (int32_t i = 0; i < n; ++i) {
+      const int32_t r = g->deg_order[i];
+      const int P = split_parts((int)(g->orow[r + 1] - g->orow[r]));
+      for (int q = 0; q < P; ++q) {
+        const RootDesc rd = root_desc(g, s, r, P > 1 ? (q | (P << 16)) : 0);
+        const int32_t* w = reinterpret_cast<const int32_t*>(&rd);
+        g->idx_desc.insert(g->idx_desc.end(), w, w + 4);
+      }
+    }
+    g->idx_extra = (int32_t)(g->idx_desc.size() / 4 - (size_t)n);
+    pin_host(g, g->idx_boff.data(), sizeof(uint32_t) * g->idx_boff.size());
+    pin_host(g, g->idx_desc.data(), sizeof(int32_t) * g->idx_desc.size());
   }
   const uint64_t total = g->idx_units;
   const size_t bytes = (size_t)total * 16;
@@ -639,18 +655,14 @@ static int ensure_index(dm_graph* g, DeviceSlot* s, LaunchCtx& ctx) {
   void* blocks = nullptr;
   uint32_t* d_boff = nullptr;
   RootDesc* desc = nullptr;
-  void* tmp = nullptr;
-  const size_t n_desc = (size_t)n + (size_t)g->idx_extra;
-  const size_t tmp_bytes = index_tables_tmp_bytes(n);
   cudaError_t e = gbuf_alloc(&blocks, std::max<size_t>(bytes, 16));
   if (e == cudaSuccess) e = gbuf_alloc(reinterpret_cast<void**>(&d_boff), sizeof(uint32_t) * std::max(n, 1));
+  const size_t n_desc = g->idx_desc.size() / 4;
   if (e == cudaSuccess) e = gbuf_alloc(reinterpret_cast<void**>(&desc), sizeof(RootDesc) * std::max<size_t>(n_desc, 1));
-  if (e == cudaSuccess) e = gbuf_alloc(&tmp, tmp_bytes);
   if (e != cudaSuccess) {
     gbuf_free(blocks, ctx.device);
     gbuf_free(d_boff, ctx.device);
     gbuf_free(desc, ctx.device);
-    gbuf_free(tmp, ctx.device);
     cudaGetLastError();
     s->index_state = -1;  // no room: per-launch bitmaps
     return DM_OK;
@@ -658,11 +670,13 @@ static int ensure_index(dm_graph* g, DeviceSlot* s, LaunchCtx& ctx) {
   s->d_blocks = blocks;
   s->d_boff = d_boff;
   s->d_desc_deg = desc;
-  s->d_index_tmp = tmp;
   s->index_bytes = bytes;
   s->index_state = 1;
-  int rc = index_tables_build(s->dg.d_odeg, s->d_deg_order, n, d_boff, desc, tmp, tmp_bytes, ctx);
-  if (rc) return rc;
+  if (n) {
+    DM_CUDA(cudaMemcpyAsync(d_boff, g->idx_boff.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice, ctx.stream));
+    DM_CUDA(cudaMemcpyAsync(desc, g->idx_desc.data(), sizeof(RootDesc) * n_desc, cudaMemcpyHostToDevice,
+                            ctx.stream));
+  }
   // roots with out-degree in [2, 256] are a contiguous range of the descending-degree order
   const int64_t lo = INDEX_MAX_DEGREE + 1 < (int64_t)g->cnt_ge.size() ? g->cnt_ge[INDEX_MAX_DEGREE + 1] : 0;
   const int64_t hi = 2 < (int64_t)g->cnt_ge.size() ? g->cnt_ge[2] : 0;

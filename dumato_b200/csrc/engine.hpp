@@ -80,19 +80,9 @@ constexpr uint32_t INDEX_NONE = 0xffffffffu;
 constexpr int INDEX_MAX_DEGREE = 256;
 constexpr int INDEX_MAX_K = 8;  // larger k rebuild the bitmaps per launch
 
-__host__ __device__ inline uint32_t index_block_units_host(int d) {
+inline uint32_t index_block_units_host(int d) {
   const int nw = (d + 63) >> 6;
   return (uint32_t)((d * nw + 1) >> 1);
-}
-
-// Entries of a root in the plain task list of the index: about d^2 / 256 for 20 to 64
-// out-neighbours (its local edges, the items, number up to d(d-1)/2), else 1. Wider roots
-// stay whole: their heavy items already split below the first level (level-1 donations), and
-// parts would stage their large blocks once per part (measured on an R-MAT graph with roots
-// of 106-171 out-neighbours: 7-cliques 70 ms whole, 79 ms in 16 parts; roots of 48-59
-// out-neighbours on another R-MAT graph: 173 µs whole, 129 µs in parts).
-__host__ __device__ inline int index_split_parts(int d) {
-  return d < 20 || d > 64 ? 1 : ((d * d + 128) / 256 > 1 ? (d * d + 128) / 256 : 1);
 }
 
 // One entry of a counting launch's task list on the index: root (rank space), out-degree,
@@ -164,12 +154,6 @@ int clique_cached_grid(const CliqueLaunch& L, LaunchCtx& ctx, int* grid);
 // Counting on the index with that grid (L.static_chunk / L.n_static set for it).
 int clique_cached_launch(const CliqueLaunch& L, LaunchCtx& ctx, int grid);
 // Builds the index blocks of roots[0..n) (rank space, 2 <= out-degree <= 64 * m).
-// The index's per-root tables built on the device from the uploaded out-degrees (rank space)
-// and descending-degree order: boff[r] (16-byte units; INDEX_NONE outside 2..256
-// out-neighbours) and the plain task list (index_split_parts entries per root, in the order).
-size_t index_tables_tmp_bytes(int n);
-int index_tables_build(const int32_t* odeg, const int32_t* deg_order, int n, uint32_t* boff, RootDesc* desc,
-                       void* tmp, size_t tmp_bytes, LaunchCtx& ctx);
 int clique_index_build(const GraphView& g, const int32_t* roots, int n, void* blocks, const uint32_t* boff, int m,
                        LaunchCtx& ctx);
 
