@@ -321,12 +321,13 @@ def batched(dm, workloads, reps: int = 2):
 
 
 def e2e_upload_bytes(g) -> int:
-    """Bytes one e2e step copies host -> device for a clique count on the index: the oriented
-    CSR (n row starts, n degrees, rows padded to multiples of 4 ints), the descending-degree
-    root order (n ints), the index block offsets (n ints), the task list (16 bytes per entry:
-    one per root, or split_parts(d) for roots of 20..64 out-neighbours, as engine.cu builds
-    it) and the 1,152-byte counter block. The DAG orients every edge from the lower to the
-    higher (degree, id) rank."""
+    """Bytes one e2e step copies host -> device for a clique count on the index: the graph's
+    clique image in one copy - the oriented CSR (n row starts, n degrees, rows padded to
+    multiples of 4 ints), the descending-degree root order (n ints), the index block offsets
+    (n ints) and the task list (16 bytes per entry: one per root, split_parts(d) for roots of
+    20..64 out-neighbours), each rounded up to 256 bytes, as engine.cu lays it out - and the
+    1,152-byte counter block. The DAG orients every edge from the lower to the higher
+    (degree, id) rank."""
     u, v = g.edges()
     n = g.info().n_vertices
     deg = np.bincount(np.concatenate([u, v]), minlength=n)
@@ -336,8 +337,10 @@ def e2e_upload_bytes(g) -> int:
     od = np.bincount(lo, minlength=n)
     padded = max(int(((od + 3) // 4 * 4).sum()), 4)
     split = (od >= 20) & (od <= 64)
-    parts = np.where(split, np.maximum(1, (od * od + 128) // 256), 1)
-    return 4 * n + 4 * n + 4 * padded + 4 * n + 4 * n + 16 * int(parts.sum()) + 1152
+    parts = int(np.where(split, np.maximum(1, (od * od + 128) // 256), 1).sum())
+    nn = max(n, 1)
+    sizes = [4 * nn, 4 * nn, 4 * padded, 4 * nn, 4 * nn, max(16 * parts, 16)]
+    return sum((b + 255) // 256 * 256 for b in sizes) + 1152
 
 
 def main():

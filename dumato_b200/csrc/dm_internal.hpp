@@ -71,6 +71,10 @@ struct dm_graph {
   std::vector<int64_t> cnt_ge;        // cnt_ge[d] = ranks with out-degree >= d
   std::vector<uint32_t> idx_boff;     // clique-index block offset per rank (16-byte units)
   std::vector<int32_t> idx_desc;      // task list of deg_order on the index, 4 ints per entry
+                                      // (kept until the clique image holds it)
+  std::vector<uint8_t> img;           // clique image: padded oriented CSR, order, index tables
+  size_t img_off[6] = {0, 0, 0, 0, 0, 0};
+  size_t img_adj_ints = 0;            // ints of the padded oriented adjacency
   int32_t idx_extra = 0;              // entries beyond one per root (roots split into parts)
   uint64_t idx_units = 0;             // 16-byte units of the whole index
   int32_t idx_maxd = 0;               // largest out-degree with a block
