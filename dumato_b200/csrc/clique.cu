@@ -68,9 +68,9 @@ static int index_build_m(const GraphView& g, const int32_t* roots, int n, void* 
                          LaunchCtx& ctx) {
   const size_t smem = (size_t)warp_layout(M).total * (CLIQUE_BLOCK / 32);
   auto kern = index_build_kernel<M>;
-  DM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  static LaunchCache cache;
   int occ = 0;
-  DM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, CLIQUE_BLOCK, smem));
+  DM_CUDA(cached_occupancy(cache, kern, ctx.device, CLIQUE_BLOCK, smem, &occ));
   if (occ < 1) return fail(DM_EINVAL, "clique index build kernel does not fit on an SM");
   const int per_grid = (n + CLIQUE_BLOCK / 32 - 1) / (CLIQUE_BLOCK / 32);
   const int grid = std::max(1, std::min(ctx.num_sms * occ, per_grid));

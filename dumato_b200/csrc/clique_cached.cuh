@@ -78,6 +78,7 @@ static __device__ __forceinline__ int load_root_chunks(const GraphView& g, int r
 // DAG only points upwards in rank).
 constexpr int INDEX_UNROLL = 4;
 
+template <int M>
 static __device__ __forceinline__ void build_rows_v4(const int32_t* adj, const int32_t* sL, const int32_t* sC,
                                                      const int32_t* sR, int d, int total, uint32_t* rows,
                                                      int row_words) {
@@ -102,10 +103,13 @@ static __device__ __forceinline__ void build_rows_v4(const int32_t* adj, const i
       const int m = own[u];
       if (m < 0) continue;
       const int32_t v[4] = {x[u].x, x[u].y, x[u].z, x[u].w};
+      // branch-free search over the members above m (out-neighbours rank above m; the last
+      // member has none): the lanes of the warp keep together whatever their candidates
+      if (m + 1 >= d) continue;
 #pragma unroll
       for (int c = 0; c < 4; ++c) {
         if (v[c] > maxL) continue;
-        const int j = lower_bound(sL, m + 1, d, v[c]);
+        const int j = m + 1 + lower_bound_bl<(M == 1 ? 64 : (M == 2 ? 128 : 256))>(sL + m + 1, d - m - 1, v[c]);
         if (j < d && sL[j] == v[c]) atomicOr(rows + m * row_words + (j >> 5), 1u << (j & 31));
       }
     }
@@ -135,7 +139,7 @@ __global__ void __launch_bounds__(256) index_build_kernel(GraphView g, const int
     const int units = (int)index_block_units(d);
     for (int i = lane; i < units * 4; i += 32) rows32[i] = 0;
     const int total = load_root_chunks(g, root, d, sL, sC, sR);
-    build_rows_v4(g.adj, sL, sC, sR, d, total, rows32, 2 * nw);
+    build_rows_v4<M>(g.adj, sL, sC, sR, d, total, rows32, 2 * nw);
     __syncwarp();
     const uint4* src = reinterpret_cast<const uint4*>(rows32);
     uint4* dst = blocks + __ldg(boff + root);
